@@ -1,0 +1,320 @@
+#!/usr/bin/env python
+"""Benchmark: DIRK3 steps/s of the 2D Euler isentropic vortex on 100,000
+periodic Voronoi cells (p=3, 40x40 blocks), FP64, GMRES(30) + block ILU(0),
+tolerance 1e-10, dt = 0.05 -- the reference's DG hot path end to end.
+
+Arms:
+  default            this library on N GPUs (one process per GPU, replicas:
+                     the path does not shard, every rank runs its own solve)
+  --impl reference   the reference's CPU path, i.e. the oracle restatement
+                     (oracle/), on this host's cores, on a bounded sample.
+
+Prints one JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DIRK3 steps/s Euler 100k-cell p3 mixed vs FP64 at 1e-8; batch solves/s, p99 ms"
+WIDTH = 10.0
+GAMMA = 1.4
+VORTEX = [5.0, 5.0, 5.0, 1.0, 1.0, GAMMA, WIDTH, WIDTH]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=100000)
+    ap.add_argument("--degree", type=int, default=3)
+    ap.add_argument("--dt", type=float, default=0.05)
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a) -> dict:
+    return {"workload": f"euler-isentropic-vortex periodic [0,10]^2, {a.cells} Voronoi cells (seed 2), p={a.degree}, "
+                        f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton 5e-13, "
+                        f"{'FP32 blocks + FGMRES' if a.precision == 'mixed' else 'FP64'}",
+            "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
+            "dt": a.dt, "gmres_m": 30, "gmres_tol": 1e-10, "preconditioner": "ilu0",
+            "precision": a.precision,
+            "l2": "inputs larger than L2: the Jacobian and ILU factors stream ~9 GB each per sweep"}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic(name: str):
+    """dram bytes per launch recorded from an ncu capture in profiles/"""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    for ln in open(p):
+        if ln.startswith("traffic_bytes_per_launch:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_sample(a, target_s: float = 12.0):
+    """Time the oracle (the reference's CPU algorithm) on a bounded sample of
+    the workload: the same problem on a smaller mesh, scaled to the full cell
+    count by the cell ratio.  Returns (steps_per_s_at_full_size, info)."""
+    import numpy as np  # noqa: F401
+
+    import cpolyg_b200 as cp
+    import oracle
+    oracle.set_threads(0)
+    threads = oracle.get_threads()
+    n = 1500 if a.degree == 3 else 3000
+    seeds = cp.uniform_seeds(2, n, WIDTH, WIDTH)
+    m = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
+    om = oracle.Mesh(m.export())
+    oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=2, dparams=VORTEX)
+    u = oe.interp(2, VORTEX)
+    st = oracle.Stepper(oe, 4, pc=2, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000)
+    t0 = time.perf_counter()
+    u = st.advance(u, a.dt, 0.0)
+    dt1 = time.perf_counter() - t0
+    info = {"sample_cells": n, "sample_seconds": dt1, "newton": int(st.stats[0]), "gmres": int(st.stats[1]),
+            "threads": threads}
+    return 1.0 / (dt1 * a.cells / n), info
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    vals = []
+    info = None
+    for k in range(a.warmup + a.steps):
+        v, info = cpu_sample(a)
+        if k >= a.warmup:
+            vals.append(v)
+    value = sum(vals) / len(vals)
+    sample = (f"one DIRK3 step of the same problem on a {info['sample_cells']}-cell mesh "
+              f"({info['sample_seconds']:.1f} s, Newton {info['newton']}, GMRES {info['gmres']} its), "
+              f"scaled by {a.cells}/{info['sample_cells']} cells")
+    out = {"metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": a.gpus,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Voronoi mesh)",
+           "config": workload(a),
+           "cpu_baseline": {"value": value, "unit": "steps/s", "cores": info["threads"], "kind": "port",
+                            "sample": sample},
+           "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(a):
+    import numpy as np
+    import torch
+
+    import cpolyg_b200 as cp
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    ctx = cp.Context(local)
+    seeds = cp.uniform_seeds(2, a.cells, WIDTH, WIDTH)
+    mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
+    eq = cp.Euler(ctx, mesh, a.degree, gamma=GAMMA, dirichlet=(cp.INIT_VORTEX, VORTEX))
+    mixed = a.precision == "mixed"
+    kw = dict(pc=cp.PC_ILU0, precision=cp.F32 if mixed else cp.F64, gmres_m=30, gmres_tol=1e-10,
+              gmres_maxit=90000, flexible=mixed)
+    stepper = cp.DIRK(3, eq, **kw)
+    u = eq.interp(cp.INIT_VORTEX, VORTEX)
+    stream = torch.cuda.current_stream()
+
+    t = 0.0
+    for _ in range(a.warmup):
+        stepper.advance(u, a.dt, t)
+        t += a.dt
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    launches0 = ctx.launches
+    newton = gmres = 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(a.steps):
+        stepper.advance(u, a.dt, t)
+        newton += stepper.stats.newton_iterations
+        gmres += stepper.stats.gmres_iterations
+        t += a.dt
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launches - launches0
+    clk = clocks.stop()
+    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.barrier()
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * a.steps / (ms_max / 1000.0)
+
+    # end to end through the C ABI with host buffers (cpg_step_host)
+    e2e = None
+    if not a.no_e2e:
+        uh = torch.empty(u.numel(), dtype=torch.float64).pin_memory().numpy()
+        uh[:] = u.cpu().numpy().ravel()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            stepper.advance_host(uh, a.dt, t)
+            t += a.dt
+        torch.cuda.synchronize()
+        e2e_s = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(e2e_s, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * a.steps / float(e2e_s.item()), "unit": "steps/s",
+               "h2d_bytes_per_step": int(uh.nbytes), "d2h_bytes_per_step": int(uh.nbytes)}
+
+    # roofline of the dominant kernel class (block-row streaming kernel:
+    # BSR matvec), timed live with CUDA events on the launching stream
+    roof = None
+    if rank == 0:
+        J = eq.jacobian(u, t, scale=-a.dt * 0.717933260754, add_mass=True,
+                        precision=cp.F32 if mixed else cp.F64)
+        x = torch.randn(u.numel(), dtype=torch.float64, device="cuda")
+        y = torch.empty_like(x)
+        for _ in range(3):
+            ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())))
+        reps = 20
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_launch = e0.elapsed_time(e1) / reps / 1000.0
+        s_a = 4 if mixed else 8
+        alg = J.nb * J.bl * J.bl * s_a + 2 * J.n_rows * J.bl * 8
+        pk = peaks()
+        ach = alg / t_launch / 1e9
+        traffic = profiled_traffic("bsr_matvec_f64_bl40.md" if not mixed else "bsr_matvec_f32_bl40.md")
+        roof = {"kernel": "k_rows (BSR matvec, 40x40 blocks)", "bound": "hbm", "achieved": ach,
+                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
+                "peak_source": pk["source"], "algorithmic_bytes": alg, "launch_ms": t_launch * 1e3,
+                "traffic": traffic}
+        del J
+
+    if rank == 0:
+        cpu = None
+        if not a.no_cpu_baseline and world == 1:
+            v, info = cpu_sample(a)
+            cpu = {"value": v, "unit": "steps/s", "cores": info["threads"], "kind": "port",
+                   "sample": (f"oracle DIRK3 step on a {info['sample_cells']}-cell mesh of the same problem "
+                              f"({info['sample_seconds']:.1f} s), scaled by cell count")}
+        out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Voronoi mesh, analytic vortex)",
+               "config": dict(workload(a), parallelism=f"replicas x{world}"),
+               "newton_iterations_per_step": newton / a.steps, "gmres_iterations_per_step": gmres / a.steps,
+               "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,113 @@
+// Internal object layouts shared by the translation units of the library.
+#pragma once
+#include <vector>
+
+#include "common.cuh"
+#include "mesh.hpp"
+#include "physics.cuh"
+
+const cpg::Mesh &cpg_mesh_ref(const cpg_mesh *m);
+
+namespace cpg {
+
+// device view of the quadrature geometry (structure of arrays)
+struct Geo {
+    int n;
+    const double4 *bb;        // x0, y0, w, h
+    const int *vq_ptr;        // n+1, volume qp range of each cell
+    const double *vx, *vy, *vxi, *veta, *vw;
+    const int *f_ptr;         // n+1, faces (= polygon edges) of each cell
+    const int *f_nbr;         // neighbour cell or boundary code
+    const int *f_blk;         // BSR block of the neighbour (or -1)
+    const double *f_nx, *f_ny;
+    const double *qx, *qy, *qxi, *qeta, *qxin, *qetan, *qw;  // face qp f*nqf+q
+};
+
+}  // namespace cpg
+
+struct cpg_equation {
+    cpg_ctx *ctx = nullptr;
+    int physics = 0, degree = 1, nb = 3, nc = 1, bl = 3, n = 0, nqf = 2;
+    double gamma = 1.4, beta[2] = {1, 1};
+    cpg::BCParams bc{};
+    int n_vqp = 0, n_faces = 0;
+    // device geometry
+    double4 *bb = nullptr;
+    int *vq_ptr = nullptr, *f_ptr = nullptr, *f_nbr = nullptr, *f_blk = nullptr;
+    double *vx = nullptr, *vy = nullptr, *vxi = nullptr, *veta = nullptr, *vw = nullptr;
+    double *f_nx = nullptr, *f_ny = nullptr;
+    double *qx = nullptr, *qy = nullptr, *qxi = nullptr, *qeta = nullptr, *qxin = nullptr, *qetan = nullptr,
+           *qw = nullptr;
+    double *mass = nullptr, *mass_inv = nullptr;  // n * nb * nb, column-major
+    double *interp_pinv = nullptr;                // nb x (p+1)^2
+    std::vector<double> gl_nodes;                 // p+1 ascending
+    // Jacobian pattern (host and device)
+    std::vector<int> rowptr, colidx;
+    int *rowptr_d = nullptr, *colidx_d = nullptr;
+    int levels_lower = 0, levels_upper = 0;
+
+    cpg::Geo geo() const {
+        return cpg::Geo{n, bb, vq_ptr, vx, vy, vxi, veta, vw, f_ptr, f_nbr, f_blk, f_nx, f_ny,
+                        qx, qy, qxi, qeta, qxin, qetan, qw};
+    }
+};
+
+struct cpg_bsr {
+    cpg_ctx *ctx = nullptr;
+    int n_rows = 0, bl = 0, precision = CPG_F64;
+    int64_t nnzb = 0;
+    std::vector<int> rowptr, colidx;   // host copies of the pattern
+    int *rowptr_d = nullptr, *colidx_d = nullptr;
+    void *vals = nullptr;              // double or float, nnzb * bl * bl
+    bool owns_pattern = true;
+    size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
+};
+
+struct cpg_precond {
+    cpg_ctx *ctx = nullptr;
+    int kind = CPG_PC_NONE, precision = CPG_F64, n = 0, bl = 0;
+    // level schedule
+    std::vector<int> lptr, lrows, uptr, urows;
+    int *lrows_d = nullptr, *urows_d = nullptr;
+    // strictly lower factor L (reference BlockILU0::L)
+    std::vector<int> L_rowptr, L_col;
+    int *L_rowptr_d = nullptr, *L_col_d = nullptr;
+    void *L_vals = nullptr;
+    // [D^{-1}_i, U_i*] rows (reference DD and DU, D^{-1} first)
+    std::vector<int> U_rowptr, U_col;
+    int *U_rowptr_d = nullptr, *U_col_d = nullptr;
+    void *U_vals = nullptr;
+    // FP64 pivot inverses used during factorisation
+    double *dinv64 = nullptr;   // only for FP32 storage (FP64 storage reads U_vals)
+    int *dinv_idx_d = nullptr;  // block index of D^{-1}_i in its FP64 array
+    // per-row factor work lists (lower neighbours ascending):
+    //   A block (j,i), A block (i,j), L block (j,i), U block (i,j)
+    std::vector<int> lp_ptr;
+    int *lp_ptr_d = nullptr, *lp_i_d = nullptr, *lp_aji_d = nullptr, *lp_aij_d = nullptr, *lp_l_d = nullptr, *lp_u_d = nullptr;
+    int *diag_a_d = nullptr;    // A block index of (i,i)
+    // A -> U position of upper blocks (only for CPG_PC_ILU0 structure checks)
+    int64_t nnzL = 0, nnzU = 0;
+    size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
+};
+
+namespace cpg {
+// linear operator + preconditioner seen by the Krylov solvers
+struct LinOp {
+    virtual cpg_status apply(cpg_ctx *ctx, const double *x, double *y) const = 0;  // y = A x
+    virtual cpg_status prec(cpg_ctx *ctx, double *x) const = 0;                    // x = P^{-1} x
+    virtual ~LinOp() {}
+};
+cpg_status gmres_op(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, double *x, int m, double tol,
+                    int maxit, int flexible, cpg_solve_stats *stats);
+// mass helpers (equation.cu)
+cpg_status mass_apply_axpy(cpg_ctx *ctx, const cpg_equation *eq, const double *x, double alpha, const double *z,
+                           double beta, double *y);
+cpg_status mass_solve_scaled(cpg_ctx *ctx, const cpg_equation *eq, const double *x, double alpha, double *y);
+// launch helpers implemented in bsr.cu / krylov.cu and used across units
+cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y);
+cpg_status vec_axpby(cpg_ctx *ctx, int64_t n, double a, const double *x, double b, double *y);
+cpg_status vec_copy(cpg_ctx *ctx, int64_t n, const double *x, double *y);
+cpg_status vec_fill(cpg_ctx *ctx, int64_t n, double v, double *y);
+// dot products / norms with deterministic reductions; results to host
+cpg_status vec_dot(cpg_ctx *ctx, int64_t n, const double *x, const double *y, double *out_host);
+}  // namespace cpg

@@ -1,0 +1,444 @@
+// Preconditioners: block ILU(0) (BlockILU0, src/Preconditioners.cpp:49-158)
+// and block Jacobi (BlockJacobi, src/Preconditioners.cpp:8-47).
+//
+// Storage mirrors the reference's three BlockMatrix objects:
+//   L  : strictly lower blocks L_ji = A_ji D_i^{-1}, row order of A;
+//   DU : per row [D_i^{-1}, U_ij = D_i^{-1} A_ij ...], row order of A;
+// Block Jacobi keeps only the D_i^{-1} rows.  Pivot blocks are inverted in
+// FP64 (partial pivoting); factors may be stored in FP32.
+//
+// Factorisation is level scheduled over the lower dependency graph of the
+// natural row order (row j depends on its lower neighbours i < j), which
+// reproduces the reference's sequential result; each level is one launch
+// with one CTA per row.  Application runs the forward sweep over the lower
+// levels and the backward sweep (fused with D^{-1}) over the upper levels.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <new>
+
+#include "internal.hpp"
+
+using namespace cpg;
+
+namespace cpg {
+cpg_status rows_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
+                   const int *col, const void *vals, const double *x, double *y, int mode);
+}
+
+namespace {
+
+enum { MODE_MATVEC = 0, MODE_FORWARD = 1, MODE_BACKWARD = 2 };
+
+// C = A * B or C -= A * B, column-major BL x BL blocks in shared memory
+__device__ __forceinline__ void smem_gemm(int BL, const double *A, const double *B, double *C, bool sub) {
+    const int n2 = BL * BL;
+    for (int o = threadIdx.x; o < n2; o += blockDim.x) {
+        const int r = o % BL, c = o / BL;
+        const double *bc = B + c * BL;
+        double s = 0.0;
+        for (int m = 0; m < BL; m++) s += A[m * BL + r] * bc[m];
+        if (sub) C[o] = C[o] - s;
+        else C[o] = s;
+    }
+}
+
+template <class T>
+__device__ __forceinline__ void load_blk(int BL, const T *src, double *dst) {
+    for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) dst[o] = (double)src[o];
+}
+template <class T>
+__device__ __forceinline__ void store_blk(int BL, const double *src, T *dst) {
+    for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) dst[o] = (T)src[o];
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting (largest magnitude,
+// lowest index on ties, as LAPACK's idamax).  Returns false on a zero pivot.
+__device__ bool smem_inverse(int BL, double *A, int *piv, double *rowp, double *fcol, int *s_ok) {
+    if (threadIdx.x == 0) *s_ok = 1;
+    __syncthreads();
+    for (int p = 0; p < BL; p++) {
+        if (threadIdx.x < 32) {
+            const int lane = threadIdx.x;
+            double best = -1.0;
+            int bi = p;
+            for (int r = p + lane; r < BL; r += 32) {
+                const double a = fabs(A[p * BL + r]);
+                if (a > best) {
+                    best = a;
+                    bi = r;
+                }
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                if (ob > best || (ob == best && oi < bi)) {
+                    best = ob;
+                    bi = oi;
+                }
+            }
+            if (lane == 0) {
+                piv[p] = bi;
+                if (!(best > 0.0)) *s_ok = 0;
+            }
+        }
+        __syncthreads();
+        const int q = piv[p];
+        if (q != p)
+            for (int c = threadIdx.x; c < BL; c += blockDim.x) {
+                const double t = A[c * BL + p];
+                A[c * BL + p] = A[c * BL + q];
+                A[c * BL + q] = t;
+            }
+        __syncthreads();
+        const double pv = A[p * BL + p];
+        const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
+        for (int c = threadIdx.x; c < BL; c += blockDim.x) rowp[c] = (c == p ? 1.0 : A[c * BL + p]) * inv;
+        for (int r = threadIdx.x; r < BL; r += blockDim.x) fcol[r] = (r == p) ? 0.0 : A[p * BL + r];
+        __syncthreads();
+        for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) {
+            const int r = o % BL, c = o / BL;
+            if (r == p) A[o] = rowp[c];
+            else A[o] = (c == p ? 0.0 : A[o]) - fcol[r] * rowp[c];
+        }
+        __syncthreads();
+    }
+    for (int p = BL - 1; p >= 0; p--) {
+        const int q = piv[p];
+        if (q != p)
+            for (int r = threadIdx.x; r < BL; r += blockDim.x) {
+                const double t = A[p * BL + r];
+                A[p * BL + r] = A[q * BL + r];
+                A[q * BL + r] = t;
+            }
+        __syncthreads();
+    }
+    return *s_ok != 0;
+}
+
+constexpr int FT = 256;  // threads per factor CTA
+
+// One CTA per row j of the level:
+//   for each lower neighbour i < j (ascending):
+//       L_ji = A_ji D_i^{-1}; Ahat_jj -= L_ji A_ij; U_ij = D_i^{-1} A_ij
+//   D_j^{-1} = inv(Ahat_jj)
+template <class TA, class TS>
+__global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict__ rows, const TA *__restrict__ A,
+                                                   const int *__restrict__ diag_a, const int *__restrict__ lp_ptr,
+                                                   const int *__restrict__ lp_i, const int *__restrict__ lp_aji,
+                                                   const int *__restrict__ lp_aij, const int *__restrict__ lp_l,
+                                                   const int *__restrict__ lp_u, TS *__restrict__ Lv,
+                                                   TS *Uv, const int *__restrict__ U_rowptr,
+                                                   double *dinv, const int *__restrict__ dinv_idx, int *flag) {
+    extern __shared__ double sm[];
+    __shared__ int s_ok;
+    const size_t b2 = (size_t)BL * BL;
+    double *Ah = sm, *D = sm + b2, *X = sm + 2 * b2, *Y = sm + 3 * b2, *T = sm + 4 * b2;
+    double *rowp = sm + 5 * b2, *fcol = rowp + BL;
+    int *piv = (int *)(fcol + BL);
+    const int j = rows ? rows[blockIdx.x] : blockIdx.x;
+    load_blk(BL, A + (size_t)diag_a[j] * b2, Ah);
+    for (int p = lp_ptr[j]; p < lp_ptr[j + 1]; p++) {
+        load_blk(BL, dinv + (size_t)dinv_idx[lp_i[p]] * b2, D);
+        load_blk(BL, A + (size_t)lp_aji[p] * b2, X);
+        load_blk(BL, A + (size_t)lp_aij[p] * b2, Y);
+        __syncthreads();
+        smem_gemm(BL, X, D, T, false);  // L_ji
+        __syncthreads();
+        store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
+        smem_gemm(BL, T, Y, Ah, true);   // Ahat_jj -= L_ji A_ij
+        smem_gemm(BL, D, Y, X, false);   // U_ij
+        __syncthreads();
+        store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
+        __syncthreads();
+    }
+    __syncthreads();
+    const bool ok = smem_inverse(BL, Ah, piv, rowp, fcol, &s_ok);
+    if (!ok && threadIdx.x == 0) {
+        atomicExch(flag, 1);
+        atomicMin(flag + 1, j);
+    }
+    double *dj = dinv + (size_t)dinv_idx[j] * b2;
+    TS *uj = Uv + (size_t)U_rowptr[j] * b2;
+    store_blk(BL, Ah, dj);
+    if ((void *)uj != (void *)dj) store_blk(BL, Ah, uj);
+}
+
+template <class TA, class TS>
+cpg_status launch_factor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
+    const int BL = P->bl;
+    const size_t smem = (5 * (size_t)BL * BL + 2 * BL) * sizeof(double) + BL * sizeof(int) + 16;
+    static int configured_max = 0;
+    if ((int)smem > 48 * 1024 && (int)smem > configured_max) {
+        CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)smem));
+        configured_max = (int)smem;
+    }
+    double *dinv = P->precision == CPG_F64 ? (double *)P->U_vals : P->dinv64;
+    k_ilu_factor<TA, TS><<<nrows, FT, smem, ctx->stream>>>(
+        BL, rows, (const TA *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
+        P->lp_u_d, (TS *)P->L_vals, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
+    return launched(ctx, "ilu factor kernel");
+}
+
+cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
+    if (nrows <= 0) return CPG_OK;
+    if (A->precision == CPG_F64 && P->precision == CPG_F64) return launch_factor<double, double>(ctx, P, A, nrows, rows);
+    if (A->precision == CPG_F64 && P->precision == CPG_F32) return launch_factor<double, float>(ctx, P, A, nrows, rows);
+    if (A->precision == CPG_F32 && P->precision == CPG_F32) return launch_factor<float, float>(ctx, P, A, nrows, rows);
+    return launch_factor<float, double>(ctx, P, A, nrows, rows);
+}
+
+void free_precond(cpg_precond *P) {
+    void *ptrs[] = {P->lrows_d, P->urows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, P->U_rowptr_d, P->U_col_d,
+                    P->U_vals, P->dinv64, P->dinv_idx_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d,
+                    P->lp_l_d, P->lp_u_d, P->diag_a_d};
+    for (void *p : ptrs) dfree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int precision, cpg_precond **out) {
+    if (!ctx || !A || !out) return CPG_ERR_INVALID_ARG;
+    if (kind != CPG_PC_NONE && kind != CPG_PC_ILU0 && kind != CPG_PC_BJACOBI)
+        return fail(ctx, CPG_ERR_INVALID_ARG, "unknown preconditioner kind");
+    if (precision != CPG_F64 && precision != CPG_F32) return fail(ctx, CPG_ERR_INVALID_ARG, "precision");
+    *out = nullptr;
+    cpg_precond *P = new (std::nothrow) cpg_precond();
+    if (!P) return fail(ctx, CPG_ERR_OOM, "host allocation");
+    P->ctx = ctx;
+    P->kind = kind;
+    P->precision = precision;
+    P->n = A->n_rows;
+    P->bl = A->bl;
+    if (kind == CPG_PC_NONE) {
+        *out = P;
+        return CPG_OK;
+    }
+    const int n = A->n_rows;
+    const std::vector<int> &rp = A->rowptr, &cl = A->colidx;
+    std::vector<int> diag_a(n, -1), a2l(A->nnzb, -1), a2u(A->nnzb, -1);
+    const bool ilu = kind == CPG_PC_ILU0;
+    P->L_rowptr.assign(1, 0);
+    P->U_rowptr.assign(1, 0);
+    for (int i = 0; i < n; i++) {
+        for (int k = rp[i]; k < rp[i + 1]; k++) {
+            if (cl[k] == i) {
+                if (diag_a[i] >= 0) {
+                    free_precond(P);
+                    delete P;
+                    return fail(ctx, CPG_ERR_INVALID_ARG, "row " + std::to_string(i) + " has two diagonal blocks");
+                }
+                diag_a[i] = k;
+            }
+            for (int k2 = k + 1; k2 < rp[i + 1] && ilu; k2++)
+                if (cl[k2] == cl[k]) {
+                    free_precond(P);
+                    delete P;
+                    return fail(ctx, CPG_ERR_INVALID_ARG, "row " + std::to_string(i) + " repeats a column");
+                }
+        }
+        if (diag_a[i] < 0) {
+            free_precond(P);
+            delete P;
+            return fail(ctx, CPG_ERR_INVALID_ARG, "row " + std::to_string(i) + " has no diagonal block");
+        }
+        // DU row: D^{-1} first, then upper blocks in A's row order
+        P->U_col.push_back(i);
+        if (ilu) {
+            for (int k = rp[i]; k < rp[i + 1]; k++) {
+                if (cl[k] < i) {
+                    a2l[k] = (int)P->L_col.size();
+                    P->L_col.push_back(cl[k]);
+                } else if (cl[k] > i) {
+                    a2u[k] = (int)P->U_col.size();
+                    P->U_col.push_back(cl[k]);
+                }
+            }
+        }
+        P->L_rowptr.push_back((int)P->L_col.size());
+        P->U_rowptr.push_back((int)P->U_col.size());
+    }
+    P->nnzL = (int64_t)P->L_col.size();
+    P->nnzU = (int64_t)P->U_col.size();
+    // factor work lists: for row j, lower neighbours i ascending with the A
+    // position of (i, j) (the reference searches row i for column j,
+    // Preconditioners.cpp:78-80; structurally symmetric patterns required)
+    std::vector<int> lp_i, lp_aji, lp_aij, lp_l, lp_u;
+    P->lp_ptr.assign(1, 0);
+    for (int j = 0; j < n; j++) {
+        std::vector<std::pair<int, int>> low;  // (i, A index of (j, i))
+        if (ilu)
+            for (int k = rp[j]; k < rp[j + 1]; k++)
+                if (cl[k] < j) low.push_back({cl[k], k});
+        std::sort(low.begin(), low.end());
+        for (auto &pr : low) {
+            const int i = pr.first;
+            int kij = -1;
+            for (int k = rp[i]; k < rp[i + 1]; k++)
+                if (cl[k] == j) {
+                    kij = k;
+                    break;
+                }
+            if (kij < 0) {
+                free_precond(P);
+                delete P;
+                return fail(ctx, CPG_ERR_INVALID_ARG,
+                            "block pattern is not structurally symmetric at (" + std::to_string(i) + "," +
+                                std::to_string(j) + ")");
+            }
+            lp_i.push_back(i);
+            lp_aji.push_back(pr.second);
+            lp_aij.push_back(kij);
+            lp_l.push_back(a2l[pr.second]);
+            lp_u.push_back(a2u[kij]);
+        }
+        P->lp_ptr.push_back((int)lp_i.size());
+    }
+    if (ilu) {
+        level_sets(n, rp, cl, P->lptr, P->lrows, P->uptr, P->urows);
+    } else {
+        P->lptr = {0, n};
+        P->uptr = {0, n};
+        P->lrows.resize(n);
+        for (int i = 0; i < n; i++) P->lrows[i] = i;
+        P->urows = P->lrows;
+    }
+    std::vector<int> dinv_idx(n);
+    for (int i = 0; i < n; i++) dinv_idx[i] = precision == CPG_F64 ? P->U_rowptr[i] : i;
+    cpg_status st = CPG_OK;
+    auto up = [&](int **dst, const std::vector<int> &src) {
+        if (st == CPG_OK) st = upload(ctx, dst, src);
+    };
+    up(&P->lrows_d, P->lrows);
+    up(&P->urows_d, P->urows);
+    up(&P->L_rowptr_d, P->L_rowptr);
+    up(&P->L_col_d, P->L_col);
+    up(&P->U_rowptr_d, P->U_rowptr);
+    up(&P->U_col_d, P->U_col);
+    up(&P->lp_ptr_d, P->lp_ptr);
+    up(&P->lp_i_d, lp_i);
+    up(&P->lp_aji_d, lp_aji);
+    up(&P->lp_aij_d, lp_aij);
+    up(&P->lp_l_d, lp_l);
+    up(&P->lp_u_d, lp_u);
+    up(&P->diag_a_d, diag_a);
+    up(&P->dinv_idx_d, dinv_idx);
+    const size_t b2 = (size_t)P->bl * P->bl;
+    if (st == CPG_OK && P->nnzL) {
+        cudaError_t e = cudaMalloc(&P->L_vals, P->nnzL * b2 * P->elem());
+        if (e != cudaSuccess) { (void)cudaGetLastError(); P->L_vals = nullptr; st = fail(ctx, CPG_ERR_OOM, "ILU L storage"); }
+    }
+    if (st == CPG_OK) {
+        cudaError_t e = cudaMalloc(&P->U_vals, P->nnzU * b2 * P->elem());
+        if (e != cudaSuccess) { (void)cudaGetLastError(); P->U_vals = nullptr; st = fail(ctx, CPG_ERR_OOM, "ILU DU storage"); }
+    }
+    if (st == CPG_OK && precision == CPG_F32) st = dmalloc(ctx, &P->dinv64, (size_t)n * b2);
+    if (st == CPG_OK) st = cpg_precond_refactor(ctx, P, A);
+    if (st != CPG_OK) {
+        free_precond(P);
+        delete P;
+        return st;
+    }
+    *out = P;
+    return CPG_OK;
+}
+
+cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A) {
+    if (!ctx || !P || !A) return CPG_ERR_INVALID_ARG;
+    if (P->kind == CPG_PC_NONE) return CPG_OK;
+    if (A->n_rows != P->n || A->bl != P->bl) return fail(ctx, CPG_ERR_INVALID_ARG, "matrix does not fit preconditioner");
+    const int init[2] = {0, INT_MAX};
+    CPG_CUDA(ctx, cudaMemcpyAsync(ctx->flag_dev, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    const int nlev = (int)P->lptr.size() - 1;
+    for (int l = 0; l < nlev; l++)
+        CPG_TRY(factor_level(ctx, P, A, P->lptr[l + 1] - P->lptr[l], P->lrows_d + P->lptr[l]));
+    int flag[2];
+    CPG_CUDA(ctx, cudaMemcpyAsync(flag, ctx->flag_dev, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
+    CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (flag[0]) return fail(ctx, CPG_ERR_SINGULAR_BLOCK, "singular pivot block at row " + std::to_string(flag[1]));
+    return CPG_OK;
+}
+
+cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+    if (!ctx || !x) return CPG_ERR_INVALID_ARG;
+    if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
+    if (P->kind == CPG_PC_ILU0) {
+        const int nl = (int)P->lptr.size() - 1;
+        for (int l = 0; l < nl; l++) {
+            const int cnt = P->lptr[l + 1] - P->lptr[l];
+            // rows without lower blocks pass through the forward sweep unchanged
+            CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->lrows_d + P->lptr[l], P->L_rowptr_d, P->L_col_d,
+                            P->L_vals, x, x, MODE_FORWARD));
+        }
+    }
+    const int nu = (int)P->uptr.size() - 1;
+    for (int l = 0; l < nu; l++) {
+        const int cnt = P->uptr[l + 1] - P->uptr[l];
+        CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->urows_d + P->uptr[l], P->U_rowptr_d, P->U_col_d,
+                        P->U_vals, x, x, MODE_BACKWARD));
+    }
+    return CPG_OK;
+}
+
+void cpg_precond_destroy(cpg_precond *P) {
+    if (!P) return;
+    cudaStreamSynchronize(P->ctx->stream);
+    free_precond(P);
+    delete P;
+}
+
+cpg_status cpg_precond_levels(const cpg_precond *P, int *n_lower, int *lower_ptr, int *lower_rows, int *n_upper,
+                              int *upper_ptr, int *upper_rows) {
+    if (!P) return CPG_ERR_INVALID_ARG;
+    if (n_lower) *n_lower = (int)P->lptr.size() - 1;
+    if (n_upper) *n_upper = (int)P->uptr.size() - 1;
+    if (lower_ptr) std::memcpy(lower_ptr, P->lptr.data(), sizeof(int) * P->lptr.size());
+    if (lower_rows) std::memcpy(lower_rows, P->lrows.data(), sizeof(int) * P->lrows.size());
+    if (upper_ptr) std::memcpy(upper_ptr, P->uptr.data(), sizeof(int) * P->uptr.size());
+    if (upper_rows) std::memcpy(upper_rows, P->urows.data(), sizeof(int) * P->urows.size());
+    return CPG_OK;
+}
+
+cpg_status cpg_precond_export(cpg_ctx *ctx, const cpg_precond *P, double *dinv_host, int *l_rowptr, int *l_col,
+                              double *l_host, int *u_rowptr, int *u_col, double *u_host) {
+    if (!ctx || !P || P->kind == CPG_PC_NONE) return CPG_ERR_INVALID_ARG;
+    const size_t b2 = (size_t)P->bl * P->bl;
+    std::vector<double> U((size_t)P->nnzU * b2), L((size_t)P->nnzL * b2);
+    auto fetch = [&](const void *src, size_t nblk, double *dst) -> cpg_status {
+        if (!nblk) return CPG_OK;
+        if (P->precision == CPG_F64) {
+            CPG_CUDA(ctx, cudaMemcpyAsync(dst, src, nblk * b2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+            CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        } else {
+            std::vector<float> f(nblk * b2);
+            CPG_CUDA(ctx, cudaMemcpyAsync(f.data(), src, nblk * b2 * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream));
+            CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            for (size_t q = 0; q < f.size(); q++) dst[q] = f[q];
+        }
+        return CPG_OK;
+    };
+    CPG_TRY(fetch(P->U_vals, P->nnzU, U.data()));
+    CPG_TRY(fetch(P->L_vals, P->nnzL, L.data()));
+    // split DU rows into D^{-1} and the strictly upper part
+    int nu = 0;
+    if (u_rowptr) u_rowptr[0] = 0;
+    for (int i = 0; i < P->n; i++) {
+        const int k0 = P->U_rowptr[i];
+        if (dinv_host) std::memcpy(dinv_host + (size_t)i * b2, U.data() + (size_t)k0 * b2, b2 * sizeof(double));
+        for (int k = k0 + 1; k < P->U_rowptr[i + 1]; k++, nu++) {
+            if (u_col) u_col[nu] = P->U_col[k];
+            if (u_host) std::memcpy(u_host + (size_t)nu * b2, U.data() + (size_t)k * b2, b2 * sizeof(double));
+        }
+        if (u_rowptr) u_rowptr[i + 1] = nu;
+    }
+    if (l_rowptr) std::memcpy(l_rowptr, P->L_rowptr.data(), sizeof(int) * P->L_rowptr.size());
+    if (l_col && P->nnzL) std::memcpy(l_col, P->L_col.data(), sizeof(int) * P->L_col.size());
+    if (l_host && P->nnzL) std::memcpy(l_host, L.data(), sizeof(double) * L.size());
+    return CPG_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+"""Time-stepper parity of the CUDA path against the oracle.
+
+Bar: relative 2-norm difference of the final coefficient vectors
+|u_gpu - u_oracle| / |u_oracle| <= 1e-11 for the FP64 path; <= 1e-8 for the
+mixed-precision path (FP32 Jacobian and ILU(0) factors, FP64 FGMRES).
+"""
+import numpy as np
+import pytest
+
+import cpolyg_b200 as cp
+import oracle
+from cases import equations, to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def l2rel(a, b):
+    a, b = np.ravel(a), np.ravel(b)
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def run_both(ctx, name, deg, kind, n, width, steps, dt, pc=cp.PC_ILU0, gm=20, gtol=1e-14, gmaxit=90000,
+             precision=cp.F64, flexible=False, reuse=0, periodic=True, init=None, codes=None, dirichlet=None,
+             inflow=None, oracle_pc=None):
+    ge, oe, _ = equations(ctx, name, deg, n=n, periodic=periodic, width=width, codes=codes, dirichlet=dirichlet,
+                          inflow=inflow)
+    kind_i, params = init
+    u0 = oe.interp(kind_i, params)
+    ostep = oracle.Stepper(oe, kind, pc=pc if oracle_pc is None else oracle_pc, gmres_m=gm, gmres_tol=gtol,
+                           gmres_maxit=gmaxit)
+    gstep = cp.TimeStepper(ge, kind=kind, pc=pc, precision=precision, gmres_m=gm, gmres_tol=gtol,
+                           gmres_maxit=gmaxit, flexible=flexible, reuse_jacobian=reuse)
+    uo = u0.copy()
+    ug = to_dev(u0).reshape(ge.np, ge.nc, ge.nb)
+    t = 0.0
+    for _ in range(steps):
+        uo = ostep.advance(uo, dt, t)
+        gstep.advance(ug, dt, t)
+        t += dt
+    return to_np(ug), uo, gstep, ostep
+
+
+GAUSS = (cp.INIT_GAUSSIAN, [100.0, 0.5, 0.5])
+
+
+@pytest.mark.parametrize("kind", [cp.STEP_FORWARD_EULER, cp.STEP_RK2, cp.STEP_RK4])
+def test_explicit_advection(ctx, kind):
+    ug, uo, _, _ = run_both(ctx, "adv_const", 2, kind, 1000, 1.0, 20, 1e-4, init=GAUSS)
+    assert l2rel(ug, uo) < 1e-11
+
+
+def test_rk4_config1_full(ctx):
+    """Periodic unit square, 1000 Voronoi cells (seed 1), p=2, velocity (1,1),
+    u0 = exp(-100 r^2), RK4 dt=1e-4, 200 steps."""
+    ug, uo, _, _ = run_both(ctx, "adv_const", 2, cp.STEP_RK4, 1000, 1.0, 200, 1e-4, init=GAUSS)
+    assert l2rel(ug, uo) < 1e-11
+
+
+def test_rk4_euler_vortex(ctx):
+    vort = (cp.INIT_VORTEX, [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0])
+    ug, uo, _, _ = run_both(ctx, "euler", 2, cp.STEP_RK4, 300, 10.0, 5, 2e-3, init=vort)
+    assert l2rel(ug, uo) < 1e-11
+
+
+VORTEX = (cp.INIT_VORTEX, [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0])
+
+
+@pytest.mark.parametrize("deg", [2, 3])
+def test_dirk3_euler_vortex(ctx, deg):
+    """Config-2 semantics at oracle size: periodic [0,10]^2, isentropic vortex
+    strength 5, DIRK3 dt=0.05, GMRES(30)+ILU(0) tol 1e-10, Newton 5e-13."""
+    ug, uo, gs, os_ = run_both(ctx, "euler", deg, cp.STEP_DIRK3, 150, 10.0, 2, 0.05, gm=30, gtol=1e-10,
+                               init=VORTEX)
+    assert gs.stats.converged == 1
+    assert l2rel(ug, uo) < 1e-11
+
+
+def test_backward_euler_and_dirk5_advection(ctx):
+    for kind in (cp.STEP_BACKWARD_EULER, cp.STEP_DIRK5):
+        ug, uo, _, _ = run_both(ctx, "adv_rot", 2, kind, 200, 1.0, 2, 0.01, gm=20, gtol=1e-12, init=GAUSS,
+                                periodic=False, dirichlet=(cp.INIT_CONSTANT, [0.0]))
+        assert l2rel(ug, uo) < 1e-11
+
+
+@pytest.mark.parametrize("kind", [cp.STEP_IRK2, cp.STEP_IRK2_INV, cp.STEP_IRK3])
+def test_irk_advection_reference_ilu(ctx, kind):
+    """IRK::advance / newAdvance with the reference's BlockILU0 on the
+    stage-coupled matrix."""
+    ug, uo, gs, _ = run_both(ctx, "adv_const", 2, kind, 150, 1.0, 2, 0.01, gm=20, gtol=1e-12, gmaxit=20000,
+                             init=GAUSS)
+    assert l2rel(ug, uo) < 1e-11
+
+
+def test_irk2_euler_stage_block_jacobi(ctx):
+    """Config-5 semantics at oracle size: 2-stage Radau IIA, slip walls at
+    y=0 and y=H, inflow at x=0, outflow at x=W, density bump in Mach-0.3 flow,
+    block Jacobi on the 48x48 cell-coupled stage blocks, GMRES(40) 1e-9."""
+    g = 1.4
+    inflow = [1.0, 0.3, 0.0, (1.0 / g) / (g - 1) + 0.5 * 0.3 ** 2]
+    codes = (cp.BC_WALL, cp.BC_OUTFLOW, cp.BC_WALL, cp.BC_INFLOW)
+    bump = (cp.INIT_DENSITY_BUMP, [0.1, 0.5, 5.0, 5.0, 0.3, g])
+    ug, uo, gs, _ = run_both(ctx, "euler", 2, cp.STEP_IRK2, 150, 10.0, 1, 0.05, pc=cp.PC_STAGE_BJACOBI, gm=40,
+                             gtol=1e-9, gmaxit=20000, init=bump, periodic=False, codes=codes,
+                             dirichlet=(cp.INIT_CONSTANT, inflow), inflow=inflow, oracle_pc=3)
+    assert gs.stats.converged == 1
+    assert l2rel(ug, uo) < 1e-11
+
+
+def test_mixed_precision_dirk3(ctx):
+    """Config-3 semantics: FP32 Jacobian and ILU(0) factors, FP64 FGMRES(30)
+    with FP64 residuals; error vs the FP64 oracle <= 1e-8."""
+    ug, uo, gs, _ = run_both(ctx, "euler", 3, cp.STEP_DIRK3, 150, 10.0, 2, 0.05, gm=30, gtol=1e-10,
+                             precision=cp.F32, flexible=True, init=VORTEX)
+    assert gs.stats.converged == 1
+    assert l2rel(ug, uo) < 1e-8
+
+
+def test_step_host_matches_device(ctx):
+    ge, oe, _ = equations(ctx, "adv_const", 2, n=300)
+    u0 = oe.interp(*GAUSS)
+    s1 = cp.RK4(ge)
+    s2 = cp.RK4(ge)
+    ud = to_dev(u0).reshape(ge.np, ge.nc, ge.nb)
+    uh = u0.copy()
+    for k in range(3):
+        s1.advance(ud, 1e-3, k * 1e-3)
+        s2.advance_host(uh, 1e-3, k * 1e-3)
+    assert np.array_equal(to_np(ud), uh)

@@ -1,0 +1,255 @@
+"""Known-answer tests that pin the oracle (the reference ships no test,
+fixture or golden vector, and cannot be built here).  Each test fixes a
+piece of the restated reference arithmetic to mathematics independent of
+this project's code: numpy's Legendre module and dense LAPACK solves,
+closed-form integrals, conservation and linearity identities, and
+temporal convergence orders."""
+import numpy as np
+import numpy.polynomial.legendre as npleg
+import pytest
+
+import cpolyg_b200 as cp
+import oracle
+from cases import mesh
+
+
+def idx_pairs(p):
+    return [(i, j) for i in range(p + 1) for j in range(p + 1 - i)]
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+def test_leg2d_matches_numpy(p):
+    rng = np.random.default_rng(p)
+    pairs = idx_pairs(p)
+    c = rng.standard_normal(len(pairs))
+    for x, y in rng.uniform(-1, 1, (20, 2)):
+        ref = sum(ck * npleg.legval(x, np.eye(p + 1)[i]) * npleg.legval(y, np.eye(p + 1)[j])
+                  for ck, (i, j) in zip(c, pairs))
+        assert abs(oracle.leg2d(x, y, p + 1, c) - ref) < 1e-13 * max(1, abs(ref))
+
+
+@pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
+def test_legder_matches_analytic(p):
+    """LegDerX/LegDerY (Legendre.cpp:34-124) give the exact derivative series."""
+    rng = np.random.default_rng(10 + p)
+    pairs = idx_pairs(p)
+    c = rng.standard_normal(len(pairs))
+    dx, dy = oracle.legder(p + 1, c)
+    for x, y in rng.uniform(-1, 1, (10, 2)):
+        ex = sum(ck * npleg.legval(x, npleg.legder(np.eye(p + 1)[i])) * npleg.legval(y, np.eye(p + 1)[j])
+                 for ck, (i, j) in zip(c, pairs))
+        ey = sum(ck * npleg.legval(x, np.eye(p + 1)[i]) * npleg.legval(y, npleg.legder(np.eye(p + 1)[j]))
+                 for ck, (i, j) in zip(c, pairs))
+        assert abs(oracle.leg2d(x, y, p + 1, dx) - ex) < 1e-12 * max(1, abs(ex))
+        assert abs(oracle.leg2d(x, y, p + 1, dy) - ey) < 1e-12 * max(1, abs(ey))
+
+
+def exact_tri_monomial(T, a, b):
+    # integral of x^a y^b over a triangle via a high-order tensor Gauss rule
+    # on the collapsed square (exact for polynomials)
+    x1, y1, x2, y2, x3, y3 = T
+    g, w = npleg.leggauss(20)
+    s = 0.5 * (g + 1)
+    tot = 0.0
+    for si, wi in zip(s, w):
+        for ti, wj in zip(s, w):
+            u, v = si * (1 - ti), si * ti
+            x = x1 + (x2 - x1) * u + (x3 - x1) * v
+            y = y1 + (y2 - y1) * u + (y3 - y1) * v
+            jac = abs((x2 - x1) * (y3 - y1) - (x3 - x1) * (y2 - y1)) * si
+            tot += 0.25 * wi * wj * jac * x ** a * y ** b
+    return tot
+
+
+@pytest.mark.parametrize("deg", [2, 4, 6, 8])
+def test_triangle_rules_exact(deg):
+    """Quadrature.cpp tables: exact for total degree <= rule degree (to the
+    tables' 14 digits)."""
+    T = [0.1, 0.2, 0.9, 0.35, 0.3, 0.8]
+    for a in range(deg + 1):
+        for b in range(deg + 1 - a):
+            ex = exact_tri_monomial(T, a, b)
+            assert abs(oracle.tri_integral(T, deg, a, b) - ex) < 5e-13
+
+
+@pytest.mark.parametrize("deg,npts", [(2, 2), (4, 4), (6, 6), (8, 10)])
+def test_line_rules_exact(deg, npts):
+    x1, y1, x2, y2 = 0.2, 0.1, 0.7, 0.9
+    L = np.hypot(x2 - x1, y2 - y1)
+    g, w = npleg.leggauss(30)
+    for a in range(2 * npts):
+        for b in range(2 * npts - a):
+            t = 0.5 * (g + 1)
+            x, y = x1 + t * (x2 - x1), y1 + t * (y2 - y1)
+            ex = 0.5 * L * np.sum(w * x ** a * y ** b)
+            assert abs(oracle.line_integral(x1, y1, x2, y2, deg, a, b) - ex) < 1e-13
+
+
+@pytest.mark.parametrize("m", [1, 2, 3, 4, 5, 8])
+def test_gauss_nodes(m):
+    assert np.allclose(oracle.gl_nodes(m), npleg.leggauss(m)[0], atol=1e-15, rtol=0)
+
+
+def rect_mesh(nx, ny, W=1.0, H=1.0, periodic=False):
+    polys = []
+    for j in range(ny):
+        for i in range(nx):
+            x0, y0, hx, hy = i * W / nx, j * H / ny, W / nx, H / ny
+            polys.append([(x0, y0), (x0 + hx, y0), (x0 + hx, y0 + hy), (x0, y0 + hy)])
+    return cp.PolyMesh.from_polygons(polys, W, H, periodic=periodic)
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_mass_matrix_rectangle_closed_form(p):
+    """Axis-aligned rectangle: M = |K| diag(1 / ((2i+1)(2j+1)))."""
+    m = rect_mesh(3, 2, 1.5, 1.0)
+    om = oracle.Mesh(m.export())
+    eq = oracle.Equation(om, 0, p)
+    M = eq.mass_blocks()
+    area = 0.5 * (1.0 / 2)
+    ref = np.diag([area / ((2 * i + 1) * (2 * j + 1)) for i, j in idx_pairs(p)])
+    for i in range(om.n):
+        assert np.abs(M[i] - ref).max() < 2e-13
+
+
+@pytest.mark.parametrize("deg", [1, 2, 3])
+def test_free_stream_preserved(deg):
+    """Constant Euler state on a periodic Voronoi mesh: zero residual."""
+    _, a, om = mesh(400, True, 1.0)
+    eq = oracle.Equation(om, 2, deg)
+    U = eq.interp(0, [1.2, 0.3, -0.4, 3.1])
+    assert np.abs(eq.assemble(U)).max() < 1e-12
+
+
+@pytest.mark.parametrize("phys", [0, 1])
+def test_advection_linearity(phys):
+    """Advection is linear: J u = assemble(u) (Equation::jacobian is exact)."""
+    _, a, om = mesh(400, phys == 0, 1.0)
+    eq = oracle.Equation(om, phys, 2, beta=(0.7, -1.1), dkind=0, dparams=[0.0])
+    u = np.random.default_rng(0).standard_normal(eq.ndof)
+    rp, cl, blk = eq.jacobian(u)
+    assert np.abs(oracle.bsr_matvec(rp, cl, blk, u) - eq.assemble(u)).max() < 1e-12 * np.abs(u).max()
+
+
+def test_euler_diagonal_blocks_match_finite_differences():
+    """Diagonal Jacobian blocks are the exact derivative of the residual
+    (off-diagonal blocks use A(u_own), the reference's approximation)."""
+    _, a, om = mesh(120, True, 10.0)
+    eq = oracle.Equation(om, 2, 2)
+    rng = np.random.default_rng(1)
+    U = eq.interp(2, [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0])
+    U = U * (1 + 0.05 * rng.standard_normal(U.size))  # cell-wise jumps
+    rp, cl, blk = eq.jacobian(U)
+    bl = eq.bl
+    for dof in [0, 5, 13, 17, 26, 40]:
+        cell, c = dof // bl, dof % bl
+        h = 1e-6 * max(1.0, abs(U[dof]))
+        e = np.zeros(U.size)
+        e[dof] = h
+        fd = (eq.assemble(U + e) - eq.assemble(U - e)) / (2 * h)
+        col = blk[rp[cell]][c]
+        assert np.abs(fd[cell * bl:(cell + 1) * bl] - col).max() < 1e-5 * np.abs(col).max()
+
+
+def test_ilu0_is_exact_lu_on_block_tridiagonal():
+    """On a 1D chain (no fill outside the pattern) ILU(0) = exact LU."""
+    rng = np.random.default_rng(2)
+    n, bl = 12, 5
+    rp, cl, blocks = [0], [], []
+    for i in range(n):
+        for j in (i, i - 1, i + 1):  # diagonal first, as the Jacobian pattern
+            if 0 <= j < n:
+                cl.append(j)
+                B = rng.standard_normal((bl, bl))
+                blocks.append(B + (4 * bl * np.eye(bl) if i == j else 0))
+        rp.append(len(cl))
+    blocks = np.array(blocks)
+    A = np.zeros((n * bl, n * bl))
+    for i in range(n):
+        for k in range(rp[i], rp[i + 1]):
+            A[i * bl:(i + 1) * bl, cl[k] * bl:(cl[k] + 1) * bl] = blocks[k].T
+    x = rng.standard_normal(n * bl)
+    z = oracle.precond_apply(2, rp, cl, blocks, x)
+    assert np.abs(z - np.linalg.solve(A, x)).max() < 1e-12 * np.abs(np.linalg.solve(A, x)).max()
+    z = oracle.precond_apply(1, rp, cl, blocks, x)  # block Jacobi = block-diagonal solve
+    for i in range(n):
+        D = blocks[rp[i]].T
+        assert np.allclose(z[i * bl:(i + 1) * bl], np.linalg.solve(D, x[i * bl:(i + 1) * bl]), rtol=1e-12,
+                           atol=1e-14)
+
+
+def test_gmres_matches_dense_solve():
+    rng = np.random.default_rng(3)
+    _, a, om = mesh(80, True, 1.0, 2)
+    eq = oracle.Equation(om, 0, 1)
+    rp, cl, _ = eq.jacobian(np.zeros(eq.ndof))
+    bl = 4
+    blocks = rng.standard_normal((len(cl), bl, bl))
+    for i in range(len(rp) - 1):
+        blocks[rp[i]] += 3 * bl * np.eye(bl)
+    n = len(rp) - 1
+    A = np.zeros((n * bl, n * bl))
+    for i in range(n):
+        for k in range(rp[i], rp[i + 1]):
+            A[i * bl:(i + 1) * bl, cl[k] * bl:(cl[k] + 1) * bl] += blocks[k].T
+    b = rng.standard_normal(n * bl)
+    for pc in (0, 1, 2):
+        x, its, res = oracle.gmres(pc, rp, cl, blocks, b, np.zeros_like(b), 20, 1e-13, 5000)
+        assert np.abs(x - np.linalg.solve(A, b)).max() < 1e-10
+        assert res < 1e-13 and its > 0
+
+
+@pytest.mark.parametrize("p", [1, 2, 3])
+def test_interp_reproduces_polynomials(p):
+    _, a, om = mesh(50, False, 1.0, 4)
+    eq = oracle.Equation(om, 0, p)
+    # projection of a constant is exact and cell-local: c0 = value, rest 0
+    u = eq.interp(0, [2.5]).reshape(om.n, -1)
+    assert np.abs(u[:, 0] - 2.5).max() < 1e-13 and np.abs(u[:, 1:]).max() < 1e-13
+    # L2 norm of 1 = sqrt(area)
+    one = eq.interp(0, [1.0])
+    assert abs(eq.l2norm(one)[0] - 1.0) < 1e-12
+
+
+def temporal_error(kind, dts, T, p=2, n=200):
+    _, a, om = mesh(n, True, 1.0, 6)
+    eq = oracle.Equation(om, 0, p, beta=(1.0, 0.5))
+    u0 = eq.interp(1, [10.0, 0.5, 0.5])
+    outs = []
+    for dt in dts:
+        st = oracle.Stepper(eq, kind, pc=2, gmres_m=30, gmres_tol=1e-14, gmres_maxit=2000, newton_tol=1e-13)
+        u, t = u0.copy(), 0.0
+        for _ in range(int(round(T / dt))):
+            u = st.advance(u, dt, t)
+            t += dt
+        outs.append(u)
+    return outs
+
+
+def test_rk4_fourth_order():
+    u = temporal_error(2, [0.004, 0.002, 0.001], 0.04)
+    r = np.linalg.norm(u[0] - u[1]) / np.linalg.norm(u[1] - u[2])
+    assert 12 < r < 22
+
+
+def test_dirk3_tableau_is_second_order():
+    """The reference's 3-stage DIRK (TimeIntegration.cpp:70-77) is Crouzeix's
+    tableau evaluated with alpha = 0.435866521508459 instead of
+    2 cos(pi/18)/sqrt(3); it meets the order-2 conditions but not
+    sum b A c = 1/6.  The oracle and the GPU keep the reference's constants,
+    so the observed temporal order is 2."""
+    a = 0.435866521508459
+    A = np.array([[(1 + a) / 2, 0, 0], [-a / 2, (1 + a) / 2, 0], [1 + a, -(1 + 2 * a), (1 + a) / 2]])
+    b = np.array([1 / 6 / a ** 2, 1 - 1 / 3 / a ** 2, 1 / 6 / a ** 2])
+    c = A.sum(1)
+    assert abs(b.sum() - 1) < 1e-15 and abs(b @ c - 0.5) < 1e-15
+    assert abs(b @ A @ c - 1 / 6) > 0.3
+    u = temporal_error(4, [0.004, 0.002, 0.001], 0.016)
+    r = np.linalg.norm(u[0] - u[1]) / np.linalg.norm(u[1] - u[2])
+    assert 3 < r < 5
+
+
+def test_radau_iia_third_order():
+    u = temporal_error(6, [0.004, 0.002, 0.001], 0.016)
+    r = np.linalg.norm(u[0] - u[1]) / np.linalg.norm(u[1] - u[2])
+    assert 6 < r < 10
