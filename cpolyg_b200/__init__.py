@@ -195,7 +195,10 @@ class Equation:
     """Equation (src/Equation.h): residual, Jacobian, mass matrix, norms."""
 
     def __init__(self, ctx: Context, msh: PolyMesh, physics: int, degree: int, gamma: float = 1.4,
-                 beta=(1.0, 1.0), dirichlet=(INIT_CONSTANT, None), inflow=None):
+                 beta=(1.0, 1.0), dirichlet=(INIT_CONSTANT, None), inflow=None, exact_jacobian: bool = False):
+        """exact_jacobian=False keeps the reference's Euler Jacobian (an inexact
+        A_x entry and own-state neighbour blocks); True uses exact derivatives
+        (same residual and converged solution, quadratic Newton)."""
         self.ctx = ctx
         self.msh = msh
         self._lib = ctx._lib
@@ -203,6 +206,7 @@ class Equation:
         d.physics = physics
         d.degree = degree
         d.gamma = gamma
+        d.exact_jacobian = int(exact_jacobian)
         d.beta[0], d.beta[1] = beta
         d.dirichlet_kind = dirichlet[0]
         for q, v in enumerate(dirichlet[1] or []):

@@ -35,7 +35,7 @@ class MeshInfo(C.Structure):
 class EquationDesc(C.Structure):
     _fields_ = [("physics", C.c_int), ("degree", C.c_int), ("gamma", C.c_double), ("beta", C.c_double * 2),
                 ("dirichlet_kind", C.c_int), ("dirichlet_params", C.c_double * 8),
-                ("inflow_state", C.c_double * 4)]
+                ("inflow_state", C.c_double * 4), ("exact_jacobian", C.c_int)]
 
 
 class EquationInfo(C.Structure):

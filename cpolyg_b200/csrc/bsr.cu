@@ -84,7 +84,9 @@ __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, cons
     for (int v = 0; v < VEC; v++) acc[v] = 0.0;
     const T *base = vals + (size_t)k0 * BL2;
     const int E = nblk * BL2;
-    int blk = 0, within = e0;
+    // the start offset may lie beyond the first block when the stride
+    // exceeds bl^2 (small blocks)
+    int blk = e0 / BL2, within = e0 % BL2;
     const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
     const double sr = (mode == MODE_MATVEC) ? 1.0 : -1.0;
 #pragma unroll 4
@@ -133,7 +135,7 @@ __global__ void __launch_bounds__(256) k_rows_dyn(int BL, int G, const int *__re
         (void)r0;
         const T *base = vals + (size_t)k0 * BL2;
         const int E = nblk * BL2;
-        int blk = 0, within = tid;
+        int blk = tid / BL2, within = tid % BL2;
         const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
         const double sr = (mode == MODE_MATVEC) ? 1.0 : -1.0;
         for (int e = tid; e < E; e += S) {
@@ -310,7 +312,7 @@ cpg_status cpg_bsr_create_host(cpg_ctx *ctx, int n_rows, int bl, const int *rowp
 
 void cpg_bsr_destroy(cpg_bsr *A) {
     if (!A) return;
-    cudaStreamSynchronize(A->ctx->stream);
+    // cudaFree synchronizes the device; the context may already be gone
     free_bsr(A);
     delete A;
 }

@@ -423,6 +423,7 @@ cpg_status with_physics(const cpg_equation *eq, F &&f) {
         case CPG_EULER: {
             Euler ph;
             ph.gamma = eq->gamma;
+            ph.exact = eq->exact_jacobian;
             return by_deg(ph);
         }
     }
@@ -531,6 +532,7 @@ cpg_status cpg_equation_create(cpg_ctx *ctx, const cpg_mesh *mm, const cpg_equat
     eq->gamma = d->gamma;
     eq->beta[0] = d->beta[0];
     eq->beta[1] = d->beta[1];
+    eq->exact_jacobian = d->exact_jacobian ? 1 : 0;
     eq->bc.dkind = d->dirichlet_kind;
     for (int q = 0; q < 8; q++) eq->bc.dparams[q] = d->dirichlet_params[q];
     for (int q = 0; q < 4; q++) eq->bc.inflow[q] = d->inflow_state[q];
@@ -736,7 +738,7 @@ cpg_status cpg_equation_create(cpg_ctx *ctx, const cpg_mesh *mm, const cpg_equat
 
 void cpg_equation_destroy(cpg_equation *eq) {
     if (!eq) return;
-    cudaStreamSynchronize(eq->ctx->stream);
+    // cudaFree synchronizes the device; the context may already be gone
     free_equation(eq);
     delete eq;
 }

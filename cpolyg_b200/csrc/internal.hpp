@@ -45,6 +45,7 @@ struct cpg_equation {
     std::vector<int> rowptr, colidx;
     int *rowptr_d = nullptr, *colidx_d = nullptr;
     int levels_lower = 0, levels_upper = 0;
+    int exact_jacobian = 0;
 
     cpg::Geo geo() const {
         return cpg::Geo{n, bb, vq_ptr, vx, vy, vxi, veta, vw, f_ptr, f_nbr, f_blk, f_nx, f_ny,

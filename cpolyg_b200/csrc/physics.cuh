@@ -97,6 +97,11 @@ struct Advection {
 struct Euler {
     static constexpr int NC = 4;
     double gamma;
+    // 0: the reference's flux Jacobians (entry (3,1) of A_x reads
+    //    H - (g-1)(u^2+v^2), Euler.cpp:154-163; neighbour blocks use the own
+    //    state, Euler.cpp:168-179); 1: exact derivatives (H - (g-1) u^2, and
+    //    A(u2), d alpha/d u2 for the neighbour blocks)
+    int exact;
     __device__ __forceinline__ void eflux(const double *U, double *fx, double *fy, double &c, double &u,
                                           double &v) const {
         const double rho = U[0], rhoU = U[1], rhoV = U[2], rhoE = U[3];
@@ -142,6 +147,7 @@ struct Euler {
         A1[4] = -u * v; A1[5] = v; A1[6] = u; A1[7] = 0;
         A1[8] = -v * v + 0.5 * (g - 1) * usq; A1[9] = -(g - 1) * u; A1[10] = (3 - g) * v; A1[11] = g - 1;
         A1[12] = v * (0.5 * (g - 1) * usq - H); A1[13] = -(g - 1) * u * v; A1[14] = H - (g - 1) * v * v; A1[15] = g * v;
+        if (exact) A0[13] = H - (g - 1) * u * u;
     }
     // alphaDerivative (Euler.cpp:35-98)
     __device__ __forceinline__ void alpha_der(const double *v1s, const double *v2s, double nx, double ny,
@@ -194,8 +200,13 @@ struct Euler {
     __device__ __forceinline__ void numfluxjac(const double *U, const double *U2, double x, double y, double nx,
                                                double ny, int sgn, double *J) const {
         double A0[16], A1[16], ap[4], alpha;
-        fluxjac(U, x, y, A0, A1);
-        alpha_der(U, U2, nx, ny, ap, alpha);
+        if (sgn < 0 && exact) {  // derivative with respect to the neighbour state
+            fluxjac(U2, x, y, A0, A1);
+            alpha_der(U2, U, nx, ny, ap, alpha);
+        } else {
+            fluxjac(U, x, y, A0, A1);
+            alpha_der(U, U2, nx, ny, ap, alpha);
+        }
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll

@@ -30,16 +30,39 @@ namespace {
 
 enum { MODE_MATVEC = 0, MODE_FORWARD = 1, MODE_BACKWARD = 2 };
 
-// C = A * B or C -= A * B, column-major BL x BL blocks in shared memory
+// C = A * B or C -= A * B, column-major BL x BL blocks in shared memory.
+// Each thread owns a 2 x 4 register tile (rows r0, r0+1; columns c0..c0+3);
+// row tiles vary fastest across a warp, so the B reads are broadcasts and the
+// A reads are consecutive doubles.
 __device__ __forceinline__ void smem_gemm(int BL, const double *A, const double *B, double *C, bool sub) {
-    const int n2 = BL * BL;
-    for (int o = threadIdx.x; o < n2; o += blockDim.x) {
-        const int r = o % BL, c = o / BL;
-        const double *bc = B + c * BL;
-        double s = 0.0;
-        for (int m = 0; m < BL; m++) s += A[m * BL + r] * bc[m];
-        if (sub) C[o] = C[o] - s;
-        else C[o] = s;
+    const int tr_n = (BL + 1) / 2, tc_n = (BL + 3) / 4;
+    for (int t = threadIdx.x; t < tr_n * tc_n; t += blockDim.x) {
+        const int r0 = 2 * (t % tr_n), c0 = 4 * (t / tr_n);
+        const bool r1ok = r0 + 1 < BL;
+        const int nc = min(4, BL - c0);
+        double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+        const double *b0 = B + c0 * BL;
+        for (int m = 0; m < BL; m++) {
+            const double a0 = A[m * BL + r0], a1 = r1ok ? A[m * BL + r0 + 1] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                const double bv = j < nc ? b0[j * BL + m] : 0.0;
+                acc[0][j] += a0 * bv;
+                acc[1][j] += a1 * bv;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (j >= nc) break;
+            double *cc = C + (c0 + j) * BL + r0;
+            if (sub) {
+                cc[0] = cc[0] - acc[0][j];
+                if (r1ok) cc[1] = cc[1] - acc[1][j];
+            } else {
+                cc[0] = acc[0][j];
+                if (r1ok) cc[1] = acc[1][j];
+            }
+        }
     }
 }
 
@@ -169,12 +192,9 @@ template <class TA, class TS>
 cpg_status launch_factor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
     const int BL = P->bl;
     const size_t smem = (5 * (size_t)BL * BL + 2 * BL) * sizeof(double) + BL * sizeof(int) + 16;
-    static int configured_max = 0;
-    if ((int)smem > 48 * 1024 && (int)smem > configured_max) {
+    if ((int)smem > 48 * 1024)  // per launch: contexts on several host threads may share the kernel
         CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
-        configured_max = (int)smem;
-    }
     double *dinv = P->precision == CPG_F64 ? (double *)P->U_vals : P->dinv64;
     k_ilu_factor<TA, TS><<<nrows, FT, smem, ctx->stream>>>(
         BL, rows, (const TA *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
@@ -386,7 +406,7 @@ cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
 
 void cpg_precond_destroy(cpg_precond *P) {
     if (!P) return;
-    cudaStreamSynchronize(P->ctx->stream);
+    // cudaFree synchronizes the device; the context may already be gone
     free_precond(P);
     delete P;
 }

@@ -663,7 +663,7 @@ cpg_status cpg_stepper_create(cpg_ctx *ctx, cpg_equation *eq, const cpg_stepper_
 
 void cpg_stepper_destroy(cpg_stepper *S) {
     if (!S) return;
-    cudaStreamSynchronize(S->ctx->stream);
+    // cudaFree synchronizes the device; the context may already be gone
     free_stepper(S);
     delete S;
 }

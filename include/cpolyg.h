@@ -195,6 +195,12 @@ typedef struct {
     int dirichlet_kind;   /* cpg_init_kind used for CPG_BC_DIRICHLET        */
     double dirichlet_params[8];
     double inflow_state[4];  /* state for CPG_BC_INFLOW                     */
+    int exact_jacobian;   /* 0: the reference's Euler Jacobian (entry (3,1)
+                             of A_x is H-(g-1)(u^2+v^2), Euler.cpp:154-163;
+                             neighbour blocks use the own state,
+                             Euler.cpp:168-179); 1: exact derivatives.  The
+                             residual, and so the converged solution, is the
+                             same; only Newton's convergence rate differs.  */
 } cpg_equation_desc;
 
 cpg_status cpg_equation_create(cpg_ctx *ctx, const cpg_mesh *m,

@@ -28,6 +28,7 @@ _PROTO = {
     "orc_mesh_export": (None, [P, PI, PI, PD, PD, PD]),
     "orc_eq_create": (P, [P, I, I, D, D, D, I, PD, PD]),
     "orc_eq_destroy": (None, [P]),
+    "orc_eq_set_exact_jacobian": (None, [P, I]),
     "orc_eq_nnzb": (I, [P]),
     "orc_assemble": (None, [P, PD, D, PD]),
     "orc_jacobian": (None, [P, PD, D, PI, PI, PD]),
@@ -130,7 +131,7 @@ class Equation:
     ADV_CONST, ADV_ROT, EULER = 0, 1, 2
 
     def __init__(self, mesh: Mesh, physics: int, degree: int, gamma=1.4, beta=(1.0, 1.0), dkind=0, dparams=None,
-                 inflow=None):
+                 inflow=None, exact_jacobian=False):
         L = load()
         self.mesh = mesh
         self.nc = 4 if physics == 2 else 1
@@ -146,6 +147,8 @@ class Equation:
             inf[: len(inflow)] = inflow
         self._keep = (dp, inf)
         self.h = L.orc_eq_create(mesh.h, physics, degree, gamma, beta[0], beta[1], dkind, pd(dp), pd(inf))
+        if exact_jacobian:
+            L.orc_eq_set_exact_jacobian(self.h, 1)
 
     @property
     def ndof(self):

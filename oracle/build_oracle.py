@@ -52,14 +52,14 @@ def build_ref() -> str | None:
     if os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(driver):
         return out
     tri_o = os.path.join(REF_OUT, "triangle.o")
-    # Triangle as a library with double precision, as src/triangle/triangle.c:213-219
-    _run(["gcc", "-O2", "-fPIC", "-DTRILIBRARY", "-DREAL=double", "-DANSI_DECLARATORS", "-DNO_TIMER",
-          "-c", tri, "-o", tri_o])
+    # Triangle: the file configures itself as a double-precision library
+    # (src/triangle/triangle.c:213-219)
+    _run(["gcc", "-O2", "-fPIC", "-DNO_TIMER", "-w", "-c", tri, "-o", tri_o])
     # Voro++ 2D: the single amalgamated translation unit of the library
     voro_o = os.path.join(REF_OUT, "voro2d.o")
-    _run(["g++", "-O2", "-fPIC", "-I", vsrc, "-c", os.path.join(vsrc, "voro++_2d.cc"), "-o", voro_o])
+    _run(["g++", "-O2", "-fPIC", "-w", "-I", vsrc, "-c", os.path.join(vsrc, "voro++_2d.cc"), "-o", voro_o])
     _run(["g++", "-O2", "-fPIC", "-shared", "-std=c++17", "-I", vsrc, "-I", os.path.join(REF_SRC, "src", "triangle"),
-          "-DANSI_DECLARATORS", "-DREAL=double", "-o", out, driver, tri_o, voro_o])
+          "-o", out, driver, tri_o, voro_o])
     return out
 
 

@@ -28,6 +28,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <unordered_map>
@@ -480,6 +481,9 @@ struct Equation {
     const Mesh *msh;
     int phys, nc, deg, nb, bl;
     double gamma, bx, by;
+    // false: neighbour blocks as the reference (A and alpha' of the own
+    // state, Euler.cpp:168-179); true: exact derivative w.r.t. the neighbour
+    bool exact_nbr = false;
     int dkind;
     double dparams[8];
     double inflow[4];
@@ -554,6 +558,9 @@ struct Equation {
                                  {v * (0.5 * (g - 1) * usq - Hh), -(g - 1) * u * v, Hh - (g - 1) * v * v, g * v}};
         std::memcpy(A[0], a0, sizeof(a0));
         std::memcpy(A[1], a1, sizeof(a1));
+        // the reference's entry (3,1) of A_x reads H - (g-1)(u^2+v^2); the
+        // derivative of (rhoE + p) u with respect to rho u is H - (g-1) u^2
+        if (exact_nbr) A[0][3][1] = Hh - (g - 1) * u * u;
     }
     // Euler::alphaDerivative (Euler.cpp:35-98)
     void alphaDerivative(const double *v1s, const double *v2s, double nx, double ny,
@@ -606,8 +613,15 @@ struct Equation {
             return;
         }
         double A[2][4][4], ap[4], alpha;
-        fluxJacobian(U, x, y, A);
-        alphaDerivative(U, U2, nx, ny, ap, alpha);
+        if (sgn < 0 && exact_nbr) {
+            // exact derivative with respect to the neighbour state U2:
+            // 0.5 [A(U2) n - alpha I + (U - U2) (d alpha / d U2)^T]
+            fluxJacobian(U2, x, y, A);
+            alphaDerivative(U2, U, nx, ny, ap, alpha);
+        } else {
+            fluxJacobian(U, x, y, A);
+            alphaDerivative(U, U2, nx, ny, ap, alpha);
+        }
         for (int r = 0; r < 4; r++)
             for (int c = 0; c < 4; c++)
                 J[r][c] = 0.5 * (A[0][r][c] * nx + A[1][r][c] * ny + (r == c ? sgn * alpha : 0.0) +
@@ -1516,6 +1530,9 @@ static void dirk_advance(Stepper &S, double *u, double dt, double t) {
             mass_matvec(*S.M, k[stage].data(), r.data());
             for (size_t q = 0; q < N; q++) r[q] = r[q] - dt * rhs[q];
             S.last_res = maxnorm(*S.eq, r.data());
+            if (std::getenv("ORC_VERBOSE"))
+                std::fprintf(stderr, "  stage %d newton %d residual %.3e gmres_total %d\n", stage, iter,
+                             S.last_res, S.gmres_its);
             if (S.last_res < S.ntol) break;
             S.newton_its++;
             BSR B;
@@ -1902,6 +1919,7 @@ orc_eq *orc_eq_create(orc_mesh *mh, int phys, int degree, double gamma, double b
     return h;
 }
 void orc_eq_destroy(orc_eq *h) { delete h; }
+void orc_eq_set_exact_jacobian(orc_eq *h, int exact) { h->e.exact_nbr = exact != 0; }
 int orc_eq_nnzb(orc_eq *h) {
     int nnzb = h->e.msh->np;
     for (auto &q : h->e.msh->p2p)

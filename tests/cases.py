@@ -40,13 +40,16 @@ def init_field(phys: int, width: float):
 
 
 def equations(ctx, name: str, degree: int, n: int = 300, periodic: bool = True, width: float = 1.0,
-              codes: tuple | None = None, dirichlet=None, inflow=None):
+              codes: tuple | None = None, dirichlet=None, inflow=None, exact_jacobian: bool = False,
+              oracle_exact: bool | None = None):
     """(gpu Equation, oracle Equation, mesh arrays)"""
     m, arrays, om = mesh(n, periodic, width, 1, codes)
     p = PHYSICS[name]
     dk, dp = dirichlet if dirichlet is not None else init_field(p["phys"], width)
-    ge = cp.Equation(ctx, m, p["phys"], degree, gamma=GAMMA, beta=p["beta"], dirichlet=(dk, dp), inflow=inflow)
-    oe = oracle.Equation(om, p["phys"], degree, gamma=GAMMA, beta=p["beta"], dkind=dk, dparams=dp, inflow=inflow)
+    ge = cp.Equation(ctx, m, p["phys"], degree, gamma=GAMMA, beta=p["beta"], dirichlet=(dk, dp), inflow=inflow,
+                     exact_jacobian=exact_jacobian)
+    oe = oracle.Equation(om, p["phys"], degree, gamma=GAMMA, beta=p["beta"], dkind=dk, dparams=dp, inflow=inflow,
+                         exact_jacobian=exact_jacobian if oracle_exact is None else oracle_exact)
     return ge, oe, arrays
 
 

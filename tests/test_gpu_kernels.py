@@ -61,6 +61,17 @@ def test_jacobian(ctx, name, deg, periodic):
     assert rel(b3, blk) < 1e-6
 
 
+@pytest.mark.parametrize("deg", [2, 3])
+def test_jacobian_exact_mode(ctx, deg):
+    """Exact Euler Jacobian (A_x entry fixed, neighbour-state derivatives)."""
+    ge, oe, _ = equations(ctx, "euler", deg, n=200, periodic=True, exact_jacobian=True)
+    u = oe.interp(cp.INIT_VORTEX, [5.0, 0.5, 0.5, 1, 1, 1.4, 1, 1])
+    rp, cl, blk = oe.jacobian(u, 0.0)
+    J = ge.jacobian(to_dev(u).reshape(ge.np, ge.nc, ge.nb), 0.0)
+    _, _, gblk = J.export()
+    assert rel(gblk, blk) < TOL
+
+
 @pytest.mark.parametrize("name,deg", [("adv_const", 2), ("euler", 3)])
 def test_mass_norm_interp(ctx, name, deg):
     ge, oe, _ = equations(ctx, name, deg, n=300, periodic=True)

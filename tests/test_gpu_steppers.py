@@ -21,9 +21,11 @@ def l2rel(a, b):
 
 def run_both(ctx, name, deg, kind, n, width, steps, dt, pc=cp.PC_ILU0, gm=20, gtol=1e-14, gmaxit=90000,
              precision=cp.F64, flexible=False, reuse=0, periodic=True, init=None, codes=None, dirichlet=None,
-             inflow=None, oracle_pc=None):
+             inflow=None, oracle_pc=None, exact=False):
+    # the oracle always runs the reference's Jacobian: an exact-Jacobian GPU
+    # run must land on the same converged solution
     ge, oe, _ = equations(ctx, name, deg, n=n, periodic=periodic, width=width, codes=codes, dirichlet=dirichlet,
-                          inflow=inflow)
+                          inflow=inflow, exact_jacobian=exact, oracle_exact=False)
     kind_i, params = init
     u0 = oe.interp(kind_i, params)
     ostep = oracle.Stepper(oe, kind, pc=pc if oracle_pc is None else oracle_pc, gmres_m=gm, gmres_tol=gtol,
@@ -75,6 +77,17 @@ def test_dirk3_euler_vortex(ctx, deg):
     assert l2rel(ug, uo) < 1e-11
 
 
+@pytest.mark.parametrize("deg", [2, 3])
+def test_dirk3_exact_jacobian_matches_reference_solution(ctx, deg):
+    """The benchmarked configuration: exact Euler Jacobian on the GPU against
+    the oracle running the reference's Jacobian; both Newton iterations
+    converge to 5e-13, so the stage solutions agree."""
+    ug, uo, gs, os_ = run_both(ctx, "euler", deg, cp.STEP_DIRK3, 150, 10.0, 2, 0.05, gm=30, gtol=1e-10,
+                               init=VORTEX, exact=True)
+    assert gs.stats.converged == 1
+    assert l2rel(ug, uo) < 1e-11
+
+
 def test_backward_euler_and_dirk5_advection(ctx):
     for kind in (cp.STEP_BACKWARD_EULER, cp.STEP_DIRK5):
         ug, uo, _, _ = run_both(ctx, "adv_rot", 2, kind, 200, 1.0, 2, 0.01, gm=20, gtol=1e-12, init=GAUSS,
@@ -110,7 +123,7 @@ def test_mixed_precision_dirk3(ctx):
     """Config-3 semantics: FP32 Jacobian and ILU(0) factors, FP64 FGMRES(30)
     with FP64 residuals; error vs the FP64 oracle <= 1e-8."""
     ug, uo, gs, _ = run_both(ctx, "euler", 3, cp.STEP_DIRK3, 150, 10.0, 2, 0.05, gm=30, gtol=1e-10,
-                             precision=cp.F32, flexible=True, init=VORTEX)
+                             precision=cp.F32, flexible=True, init=VORTEX, exact=True)
     assert gs.stats.converged == 1
     assert l2rel(ug, uo) < 1e-8
 

@@ -151,6 +151,52 @@ def test_euler_diagonal_blocks_match_finite_differences():
         assert np.abs(fd[cell * bl:(cell + 1) * bl] - col).max() < 1e-5 * np.abs(col).max()
 
 
+def test_euler_jacobian_defect_and_exact_mode():
+    """The reference's A_x entry (3,1) is H - (g-1)(u^2+v^2) (Euler.cpp:154-163)
+    where d((rhoE+p)u)/d(rho u) = H - (g-1)u^2; on a smooth state its
+    Jacobian is therefore a few percent off.  The exact mode (that entry
+    fixed, neighbour blocks differentiated with respect to the neighbour
+    state) matches finite differences in every block."""
+    _, a, om = mesh(150, True, 10.0)
+    V = [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0]
+    errs = {}
+    for exact in (False, True):
+        eq = oracle.Equation(om, 2, 2, dkind=2, dparams=V, exact_jacobian=exact)
+        U = eq.interp(2, V)
+        rp, cl, blk = eq.jacobian(U)
+        n, bl = eq.n, eq.bl
+        worst = 0.0
+        for dof in np.random.default_rng(0).choice(n * bl, 10, replace=False):
+            h = 1e-7
+            e = np.zeros(n * bl)
+            e[dof] = h
+            fd = (eq.assemble(U + e) - eq.assemble(U - e)) / (2 * h)
+            col = np.zeros(n * bl)
+            cell, c = dof // bl, dof % bl
+            for i in range(n):
+                for k in range(rp[i], rp[i + 1]):
+                    if cl[k] == cell:
+                        col[i * bl:(i + 1) * bl] = blk[k][c]
+            worst = max(worst, np.abs(fd - col).max() / np.abs(col).max())
+        errs[exact] = worst
+    assert errs[True] < 1e-6
+    assert errs[False] > 1e-3
+
+
+def test_exact_jacobian_converges_to_the_same_solution():
+    """Newton with exact or reference Jacobians converges to the same stage
+    values (the residual is unchanged); the exact one in fewer iterations."""
+    _, a, om = mesh(300, True, 10.0, 2)
+    V = [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0]
+    out = {}
+    for exact in (False, True):
+        eq = oracle.Equation(om, 2, 2, dkind=2, dparams=V, exact_jacobian=exact)
+        st = oracle.Stepper(eq, 4, pc=2, gmres_m=30, gmres_tol=1e-10)
+        out[exact] = (st.advance(eq.interp(2, V), 0.05), int(st.stats[0]))
+    assert np.linalg.norm(out[True][0] - out[False][0]) / np.linalg.norm(out[False][0]) < 1e-11
+    assert out[True][1] < out[False][1]
+
+
 def test_ilu0_is_exact_lu_on_block_tridiagonal():
     """On a 1D chain (no fill outside the pattern) ILU(0) = exact LU."""
     rng = np.random.default_rng(2)
