@@ -142,7 +142,7 @@ def cpu_sample(a, target_s: float = 12.0):
     import oracle
     oracle.set_threads(0)
     threads = oracle.get_threads()
-    n = 1500 if a.degree == 3 else 3000
+    n = 600 if a.degree == 3 else 1500
     seeds = cp.uniform_seeds(2, n, WIDTH, WIDTH)
     m = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
     om = oracle.Mesh(m.export())
