@@ -42,13 +42,34 @@ def parse():
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--workload", default="dirk3", choices=["dirk3", "irk"],
+                    help="dirk3: the 100k-cell vortex (default); irk: 2-stage Radau IIA, 500k cells, walls/inflow/"
+                         "outflow, stage block-Jacobi GMRES(40) 1e-9")
+    ap.add_argument("--compare-fp64", type=int, default=0,
+                    help="with --precision mixed: steps over which to measure the error against the FP64 path")
+    a = ap.parse_args()
+    if a.workload == "irk":
+        if a.cells == 100000:
+            a.cells = 500000
+        if a.degree == 3:
+            a.degree = 2
+        if a.dt == 0.05:
+            a.dt = 0.02
+    return a
 
 
 def workload(a) -> dict:
+    prec = 'FP32 blocks + FGMRES' if a.precision == 'mixed' else 'FP64'
+    if a.workload == "irk":
+        return {"workload": f"euler-density-bump Mach 0.3, [0,10]^2 slip walls / inflow / outflow, {a.cells} Voronoi "
+                            f"cells (seed 5), p={a.degree}, 2-stage Radau IIA dt={a.dt}, GMRES(40) + block Jacobi on "
+                            f"48x48 cell-coupled stage blocks tol 1e-9, Newton 5e-13, {prec}",
+                "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
+                "dt": a.dt, "gmres_m": 40, "gmres_tol": 1e-9, "preconditioner": "stage block Jacobi",
+                "precision": a.precision, "jacobian": "exact",
+                "l2": "inputs larger than L2: each stage Jacobian streams ~16 GB per matvec"}
     return {"workload": f"euler-isentropic-vortex periodic [0,10]^2, {a.cells} Voronoi cells (seed 2), p={a.degree}, "
-                        f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton 5e-13, "
-                        f"{'FP32 blocks + FGMRES' if a.precision == 'mixed' else 'FP64'}",
+                        f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton 5e-13, {prec}",
             "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
             "dt": a.dt, "gmres_m": 30, "gmres_tol": 1e-10, "preconditioner": "ilu0",
             "precision": a.precision,
@@ -143,12 +164,22 @@ def cpu_sample(a, target_s: float = 12.0):
     oracle.set_threads(0)
     threads = oracle.get_threads()
     n = 600 if a.degree == 3 else 1500
-    seeds = cp.uniform_seeds(2, n, WIDTH, WIDTH)
-    m = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
-    om = oracle.Mesh(m.export())
-    oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=2, dparams=VORTEX)
-    u = oe.interp(2, VORTEX)
-    st = oracle.Stepper(oe, 4, pc=2, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000)
+    if a.workload == "irk":
+        inflow = [1.0, 0.3, 0.0, (1.0 / GAMMA) / (GAMMA - 1) + 0.5 * 0.3 ** 2]
+        codes = [cp.BC_WALL, cp.BC_OUTFLOW, cp.BC_WALL, cp.BC_INFLOW]
+        m = cp.PolyMesh.voronoi(cp.uniform_seeds(5, n, WIDTH, WIDTH), WIDTH, WIDTH, periodic=False,
+                                side_codes=codes)
+        om = oracle.Mesh(m.export(), side_codes=codes)
+        oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=0, dparams=inflow, inflow=inflow)
+        u = oe.interp(3, [0.1, 0.5, 5.0, 5.0, 0.3, GAMMA])
+        st = oracle.Stepper(oe, 6, pc=3, gmres_m=40, gmres_tol=1e-9, gmres_maxit=20000)
+    else:
+        seeds = cp.uniform_seeds(2, n, WIDTH, WIDTH)
+        m = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
+        om = oracle.Mesh(m.export())
+        oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=2, dparams=VORTEX)
+        u = oe.interp(2, VORTEX)
+        st = oracle.Stepper(oe, 4, pc=2, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000)
     t0 = time.perf_counter()
     u = st.advance(u, a.dt, 0.0)
     dt1 = time.perf_counter() - t0
@@ -181,6 +212,35 @@ def run_reference(a):
     print(json.dumps(out), flush=True)
 
 
+# ------------------------------------------------------------------ problems
+def build_problem(a, cp, ctx):
+    """(equation, stepper factory(mixed), initial state) of the workload."""
+    if a.workload == "irk":
+        # 2-stage Radau IIA on [0,10]^2: slip walls y=0,10, inflow x=0,
+        # outflow x=10; uniform Mach 0.3 flow with a density bump
+        inflow = [1.0, 0.3, 0.0, (1.0 / GAMMA) / (GAMMA - 1) + 0.5 * 0.3 ** 2]
+        codes = [cp.BC_WALL, cp.BC_OUTFLOW, cp.BC_WALL, cp.BC_INFLOW]
+        seeds = cp.uniform_seeds(5, a.cells, WIDTH, WIDTH)
+        mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=False, side_codes=codes)
+        eq = cp.Euler(ctx, mesh, a.degree, gamma=GAMMA, dirichlet=(cp.INIT_CONSTANT, inflow), inflow=inflow,
+                      exact_jacobian=True)
+        u0 = eq.interp(cp.INIT_DENSITY_BUMP, [0.1, 0.5, 5.0, 5.0, 0.3, GAMMA])
+
+        def make(mixed):
+            return cp.IRK(2, eq, pc=cp.PC_STAGE_BJACOBI, precision=cp.F32 if mixed else cp.F64, gmres_m=40,
+                          gmres_tol=1e-9, gmres_maxit=20000, flexible=mixed)
+        return eq, make, u0
+    seeds = cp.uniform_seeds(2, a.cells, WIDTH, WIDTH)
+    mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
+    eq = cp.Euler(ctx, mesh, a.degree, gamma=GAMMA, dirichlet=(cp.INIT_VORTEX, VORTEX), exact_jacobian=True)
+    u0 = eq.interp(cp.INIT_VORTEX, VORTEX)
+
+    def make(mixed):
+        return cp.DIRK(3, eq, pc=cp.PC_ILU0, precision=cp.F32 if mixed else cp.F64, gmres_m=30, gmres_tol=1e-10,
+                       gmres_maxit=90000, flexible=mixed)
+    return eq, make, u0
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_ours(a):
     import numpy as np
@@ -200,15 +260,25 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     ctx = cp.Context(local)
-    seeds = cp.uniform_seeds(2, a.cells, WIDTH, WIDTH)
-    mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
-    eq = cp.Euler(ctx, mesh, a.degree, gamma=GAMMA, dirichlet=(cp.INIT_VORTEX, VORTEX), exact_jacobian=True)
     mixed = a.precision == "mixed"
-    kw = dict(pc=cp.PC_ILU0, precision=cp.F32 if mixed else cp.F64, gmres_m=30, gmres_tol=1e-10,
-              gmres_maxit=90000, flexible=mixed)
-    stepper = cp.DIRK(3, eq, **kw)
-    u = eq.interp(cp.INIT_VORTEX, VORTEX)
+    eq, make_stepper, u0 = build_problem(a, cp, ctx)
+    stepper = make_stepper(mixed)
+    u = u0.clone()
     stream = torch.cuda.current_stream()
+
+    # mixed precision: error against the FP64 GPU path from the same state
+    err_fp64 = None
+    if mixed and a.compare_fp64 and rank == 0:
+        ref_stepper = make_stepper(False)
+        ua, ub = u0.clone(), u0.clone()
+        tt = 0.0
+        for _ in range(a.compare_fp64):
+            ref_stepper.advance(ua, a.dt, tt)
+            stepper.advance(ub, a.dt, tt)
+            tt += a.dt
+        err_fp64 = float(torch.linalg.norm(ub - ua) / torch.linalg.norm(ua))
+        del ref_stepper, ua, ub
+        torch.cuda.empty_cache()
 
     t = 0.0
     for _ in range(a.warmup):
@@ -273,18 +343,21 @@ def run_ours(a):
             ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())))
         reps = 20
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("roofline_matvec")  # lets ncu select exactly these launches
         e0.record(stream)
         for _ in range(reps):
             ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())))
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         t_launch = e0.elapsed_time(e1) / reps / 1000.0
         s_a = 4 if mixed else 8
         alg = J.nb * J.bl * J.bl * s_a + 2 * J.n_rows * J.bl * 8
         pk = peaks()
         ach = alg / t_launch / 1e9
-        traffic = profiled_traffic("bsr_matvec_f64_bl40.md" if not mixed else "bsr_matvec_f32_bl40.md")
-        roof = {"kernel": "k_rows (BSR matvec, 40x40 blocks)", "bound": "hbm", "achieved": ach,
+        traffic = profiled_traffic(f"bsr_matvec_{'f32' if mixed else 'f64'}_bl{J.bl}.md")
+        roof = {"kernel": f"k_rows (BSR matvec, {J.bl}x{J.bl} {'FP32' if mixed else 'FP64'} blocks)",
+                "bound": "hbm", "achieved": ach,
                 "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
                 "peak_source": pk["source"], "algorithmic_bytes": alg, "launch_ms": t_launch * 1e3,
                 "traffic": traffic}
@@ -295,14 +368,19 @@ def run_ours(a):
         if not a.no_cpu_baseline and world == 1:
             v, info = cpu_sample(a)
             cpu = {"value": v, "unit": "steps/s", "cores": info["threads"], "kind": "port",
-                   "sample": (f"oracle DIRK3 step on a {info['sample_cells']}-cell mesh of the same problem "
-                              f"({info['sample_seconds']:.1f} s), scaled by cell count")}
+                   "sample": (f"oracle step on a {info['sample_cells']}-cell mesh of the same problem "
+                              f"({info['sample_seconds']:.1f} s, Newton {info['newton']}, GMRES {info['gmres']} "
+                              f"its), scaled by cell count")}
         out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Voronoi mesh, analytic vortex)",
+               "vs_baseline": None, "dtype": "f32 blocks, f64 vectors" if mixed else "f64",
+               "data": "synthetic (seeded Voronoi mesh, analytic initial data)",
                "config": dict(workload(a), parallelism=f"replicas x{world}"),
                "newton_iterations_per_step": newton / a.steps, "gmres_iterations_per_step": gmres / a.steps,
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
+        if err_fp64 is not None:
+            out["error_vs_fp64"] = {"value": err_fp64, "steps": a.compare_fp64,
+                                    "norm": "relative 2-norm of the coefficient vector"}
         print(json.dumps(out), flush=True)
     ctx.close()
     if dist:
