@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 
 #include "internal.hpp"
@@ -867,6 +868,75 @@ cpg_status cpg_interp(cpg_ctx *ctx, const cpg_equation *eq, int kind, const doub
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// L2 norm without any allocation.
+//
+// cpg_l2norm keeps its partial sums in the context's scratch buffer and reads
+// the result back through a pinned host buffer; both are allocated (or grown)
+// on demand.  A caller that hands all of the device memory to its own pool --
+// the serving loop, for instance, admits each solve against a fixed memory
+// budget -- or that may not allocate inside its Newton loop can use
+// cpg_l2norm_noalloc instead: its partial sums live in the file-scope device
+// array below, which every GPU that loads this library holds until the
+// process exits, and the result is copied straight into the caller's host
+// array.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int L2_NOALLOC_MAX_NC = 4;  // components a call may reduce
+// 4 partial-sum slots per reduction CTA (k_l2_partial) plus the 4 totals
+constexpr int L2_NOALLOC_DOUBLES = RED_CTAS * 4 + 4;  // 1028 doubles, 8224 bytes
+static __device__ __align__(256) double g_l2_noalloc[L2_NOALLOC_DOUBLES];
+std::mutex g_l2_noalloc_mu;
+double *g_l2_noalloc_addr[128] = {};  // device address of the array, per device
+}  // namespace
+
+extern "C" cpg_status cpg_l2norm_noalloc(cpg_ctx *ctx, const cpg_equation *eq, const double *u, double *out_host) {
+    if (!ctx || !eq || !u || !out_host) return CPG_ERR_INVALID_ARG;
+    const size_t need = (size_t)RED_CTAS * 4 + (size_t)eq->nc;
+    if (eq->nc > L2_NOALLOC_MAX_NC || need > (size_t)L2_NOALLOC_DOUBLES)
+        return fail(ctx, CPG_ERR_INVALID_ARG,
+                    "cpg_l2norm_noalloc: " + std::to_string(eq->nc) + " components need " + std::to_string(need) +
+                        " doubles of static scratch; the maximum is " + std::to_string(L2_NOALLOC_DOUBLES) +
+                        " doubles (" + std::to_string(L2_NOALLOC_MAX_NC) + " components)");
+    if (eq->nb != 3 && eq->nb != 6 && eq->nb != 10) return fail(ctx, CPG_ERR_UNSUPPORTED, "basis size");
+    int dev = -1;
+    CPG_CUDA(ctx, cudaGetDevice(&dev));
+    if (dev != ctx->device || dev < 0 || dev >= 128)
+        return fail(ctx, CPG_ERR_INVALID_ARG, "cpg_l2norm_noalloc: make the context's device current");
+    double *part = nullptr;
+    {
+        // set-up, once per device, with that device current: the host-side
+        // name of the array is not a device address
+        std::lock_guard<std::mutex> lock(g_l2_noalloc_mu);
+        if (!g_l2_noalloc_addr[dev]) {
+            void *p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_l2_noalloc);
+            if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress of the static norm scratch");
+            g_l2_noalloc_addr[dev] = (double *)p;
+        }
+        part = g_l2_noalloc_addr[dev];
+    }
+    // every slot read below is written earlier in the same call, so nothing
+    // needs clearing; calls that overlap on the GPU share the array and race
+    switch (eq->nb) {
+        case 3: k_l2_partial<3><<<RED_CTAS, 256, 0, ctx->stream>>>(eq->n, eq->nc, eq->mass, u, part); break;
+        case 6: k_l2_partial<6><<<RED_CTAS, 256, 0, ctx->stream>>>(eq->n, eq->nc, eq->mass, u, part); break;
+        default: k_l2_partial<10><<<RED_CTAS, 256, 0, ctx->stream>>>(eq->n, eq->nc, eq->mass, u, part); break;
+    }
+    CPG_TRY(launched(ctx, "l2 partial kernel (static scratch)"));
+    k_l2_final<<<1, 32, 0, ctx->stream>>>(RED_CTAS, part, part + RED_CTAS * 4);
+    CPG_TRY(launched(ctx, "l2 final kernel (static scratch)"));
+    double sums[L2_NOALLOC_MAX_NC];
+    CPG_CUDA(ctx, cudaMemcpyAsync(sums, part + RED_CTAS * 4, sizeof(double) * eq->nc, cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int c = 0; c < eq->nc; c++) {
+        if (!std::isfinite(sums[c])) return fail(ctx, CPG_ERR_NONFINITE, "non-finite L2 norm");
+        out_host[c] = std::sqrt(std::max(0.0, sums[c]));
+    }
+    return CPG_OK;
+}
 
 namespace cpg {
 // y = alpha * M x + beta * z (Newton residual r = M k - dt b)

@@ -231,6 +231,21 @@ cpg_status cpg_mass_solve(cpg_ctx *ctx, const cpg_equation *eq,
  * out_host[nc].                                                             */
 cpg_status cpg_l2norm(cpg_ctx *ctx, const cpg_equation *eq,
                       const double *u_dev, double *out_host);
+/* No counterpart in the reference.  Same result as cpg_l2norm, for callers
+ * that may not allocate device or pinned host memory during the call:
+ * applications that give every byte of device memory to their own pool, or
+ * that admit work against a fixed memory budget (as cpolyg_b200.serve does),
+ * cannot let a norm grow a scratch buffer inside their Newton loop.  The
+ * partial sums live in a static device array of 1028 doubles (8224 bytes)
+ * that every GPU loading this library holds until the process exits; it
+ * serves equations with at most 4 components and rejects anything larger
+ * with CPG_ERR_INVALID_ARG.  The context's device must be current.  The first
+ * call on a device looks up the array's device address (set-up); make that
+ * first call before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU (several contexts or streams at once) race and must be
+ * serialized by the caller.                                                 */
+cpg_status cpg_l2norm_noalloc(cpg_ctx *ctx, const cpg_equation *eq,
+                              const double *u_dev, double *out_host);
 /* MeshFn::interp (src/MeshFn.cpp:56-145): least-squares projection on the
  * (p+1)^2 Gauss grid of each bounding box of an analytic field.             */
 cpg_status cpg_interp(cpg_ctx *ctx, const cpg_equation *eq, int init_kind,
