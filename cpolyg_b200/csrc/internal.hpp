@@ -86,7 +86,11 @@ struct cpg_precond {
     std::vector<int> lp_ptr;
     int *lp_ptr_d = nullptr, *lp_i_d = nullptr, *lp_aji_d = nullptr, *lp_aij_d = nullptr, *lp_l_d = nullptr, *lp_u_d = nullptr;
     int *diag_a_d = nullptr;    // A block index of (i,i)
-    // A -> U position of upper blocks (only for CPG_PC_ILU0 structure checks)
+    // sync-free sweeps (one launch per triangular solve): per-row publish
+    // flags and the generation counter that makes earlier values stale
+    bool syncfree = false;
+    int *row_flags_d = nullptr;
+    mutable int generation = 0;
     int64_t nnzL = 0, nnzU = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
 };
@@ -106,6 +110,17 @@ cpg_status mass_apply_axpy(cpg_ctx *ctx, const cpg_equation *eq, const double *x
 cpg_status mass_solve_scaled(cpg_ctx *ctx, const cpg_equation *eq, const double *x, double alpha, double *y);
 // launch helpers implemented in bsr.cu / krylov.cu and used across units
 cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y);
+// sync-free triangular sweep over the rows in `order` (bsr.cu)
+cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
+                    const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
+                    int *err);
+bool sweep_supported(int bl);
+// x = P^{-1} x without the host-side check of the sweep status word, for
+// callers that check once per solve (precond.cu)
+cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x);
+// reads and clears the sweep status word; a bounded wait that ran out turns
+// `st` into CPG_ERR_TIMEOUT (precond.cu)
+cpg_status check_sweep_error(cpg_ctx *ctx, cpg_status st);
 cpg_status vec_axpby(cpg_ctx *ctx, int64_t n, double a, const double *x, double b, double *y);
 cpg_status vec_copy(cpg_ctx *ctx, int64_t n, const double *x, double *y);
 cpg_status vec_fill(cpg_ctx *ctx, int64_t n, double v, double *y);

@@ -207,12 +207,12 @@ struct KrylovOp : LinOp {
     const cpg_precond *P;
     KrylovOp(const cpg_bsr *a, const cpg_precond *p) : A(a), P(p) {}
     cpg_status apply(cpg_ctx *ctx, const double *x, double *y) const override { return bsr_matvec_raw(ctx, A, x, y); }
-    cpg_status prec(cpg_ctx *ctx, double *x) const override { return cpg_precond_apply(ctx, P, x); }
+    cpg_status prec(cpg_ctx *ctx, double *x) const override { return precond_apply_raw(ctx, P, x); }
 };
 
-namespace cpg {
-cpg_status gmres_op(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, double *x, int m, double tol,
-                    int maxit, int flexible, cpg_solve_stats *stats) {
+namespace {
+cpg_status gmres_run(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, double *x, int m, double tol,
+                     int maxit, int flexible, cpg_solve_stats *stats) {
     if (m < 1 || m > 62) return fail(ctx, CPG_ERR_INVALID_ARG, "GMRES restart must be 1..62");
     // workspace: V (m+1) N, r N, [Z m N]
     const size_t need = (size_t)(m + 2 + (flexible ? m : 0)) * N;
@@ -325,6 +325,15 @@ cpg_status gmres_op(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, d
     }
     return CPG_OK;
 }
+}  // namespace
+
+namespace cpg {
+// one status check per solve: a triangular sweep whose bounded wait ran out
+// turns the whole solve into CPG_ERR_TIMEOUT
+cpg_status gmres_op(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, double *x, int m, double tol,
+                    int maxit, int flexible, cpg_solve_stats *stats) {
+    return check_sweep_error(ctx, gmres_run(ctx, op, N, b, x, m, tol, maxit, flexible, stats));
+}
 }  // namespace cpg
 
 extern "C" {
@@ -337,9 +346,11 @@ cpg_status cpg_gmres(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const
     return gmres_op(ctx, op, (int64_t)A->n_rows * A->bl, b, x, m, tol, maxit, flexible, stats);
 }
 
-cpg_status cpg_jacobi_solve(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const double *b, double *x,
-                            double tol, int maxit, cpg_solve_stats *stats) {
-    if (!ctx || !A || !P || !b || !x) return CPG_ERR_INVALID_ARG;
+}  // extern "C"
+
+namespace {
+cpg_status jacobi_run(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const double *b, double *x,
+                      double tol, int maxit, cpg_solve_stats *stats) {
     const int64_t N = (int64_t)A->n_rows * A->bl;
     double *ws;
     CPG_TRY(kws(ctx, 3 * (size_t)N, &ws));
@@ -348,7 +359,7 @@ cpg_status cpg_jacobi_solve(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P
     CPG_TRY(scratch(ctx, RED + 8, &sc));
     const double omega = 1.0;
     CPG_TRY(vec_copy(ctx, N, b, dinvb));
-    CPG_TRY(cpg_precond_apply(ctx, P, dinvb));
+    CPG_TRY(precond_apply_raw(ctx, P, dinvb));
     int mm;
     double nr = 0.0;
     for (mm = 0; mm < maxit; mm++) {
@@ -359,7 +370,7 @@ cpg_status cpg_jacobi_solve(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P
         CPG_TRY(read_host(ctx, sc + RED, 1, &nr));
         if (!std::isfinite(nr)) return fail(ctx, CPG_ERR_NONFINITE, "non-finite Jacobi residual");
         if (nr < tol) break;
-        CPG_TRY(cpg_precond_apply(ctx, P, t));
+        CPG_TRY(precond_apply_raw(ctx, P, t));
         k_jacobi_update<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, omega, dinvb, t, x);
         CPG_TRY(launched(ctx, "jacobi update kernel"));
     }
@@ -369,6 +380,15 @@ cpg_status cpg_jacobi_solve(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P
         stats->converged = nr < tol ? 1 : 0;
     }
     return CPG_OK;
+}
+}  // namespace
+
+extern "C" {
+
+cpg_status cpg_jacobi_solve(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const double *b, double *x,
+                            double tol, int maxit, cpg_solve_stats *stats) {
+    if (!ctx || !A || !P || !b || !x) return CPG_ERR_INVALID_ARG;
+    return check_sweep_error(ctx, jacobi_run(ctx, A, P, b, x, tol, maxit, stats));
 }
 
 cpg_status cpg_axpby(cpg_ctx *ctx, int64_t n, double a, const double *x, double b, double *y) {

@@ -10,10 +10,13 @@
 // Factorisation is level scheduled over the lower dependency graph of the
 // natural row order (row j depends on its lower neighbours i < j), which
 // reproduces the reference's sequential result; each level is one launch
-// with one CTA per row.  Application runs the forward sweep over the lower
-// levels and the backward sweep (fused with D^{-1}) over the upper levels.
+// with one CTA per row.  Application runs the forward sweep and the backward
+// sweep (fused with D^{-1}) either as one sync-free launch each (rows claimed
+// in level order, per-row publish flags; block sizes 6, 10, 24, 40) or as one
+// launch per level (other block sizes, or CPG_ILU_SWEEP=levels).
 #include <algorithm>
 #include <climits>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 
@@ -66,6 +69,40 @@ __device__ __forceinline__ void smem_gemm(int BL, const double *A, const double 
     }
 }
 
+// The same product on the FP64 tensor-core path (DMMA, mma.sync m8n8k4 f64;
+// the 5th-generation tcgen05 MMA has no FP64 kind), for block sizes that are
+// multiples of 8.  Each warp owns 8x8 output tiles and walks k in steps of
+// four.  Fragments: A(g, t), B(t, g), C(g, 2t) and C(g, 2t+1) with
+// g = lane / 4, t = lane % 4.
+__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+__device__ __forceinline__ void smem_gemm_dmma(int BL, const double *A, const double *B, double *C, bool sub) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int nt = BL >> 3;
+    for (int tile = warp; tile < nt * nt; tile += nw) {  // warp-uniform: all lanes issue the MMA
+        const int r0 = (tile % nt) * 8, c0 = (tile / nt) * 8;
+        double d0 = 0.0, d1 = 0.0;
+        for (int k = 0; k < BL; k += 4)
+            dmma_m8n8k4(d0, d1, A[(k + t) * BL + r0 + g], B[(c0 + g) * BL + k + t]);
+        double *cc = C + (size_t)(c0 + 2 * t) * BL + r0 + g;
+        if (sub) {
+            cc[0] = cc[0] - d0;
+            cc[BL] = cc[BL] - d1;
+        } else {
+            cc[0] = d0;
+            cc[BL] = d1;
+        }
+    }
+}
+__device__ __forceinline__ void block_gemm(int BL, const double *A, const double *B, double *C, bool sub) {
+    if ((BL & 7) == 0) smem_gemm_dmma(BL, A, B, C, sub);
+    else smem_gemm(BL, A, B, C, sub);
+}
+
 template <class T>
 __device__ __forceinline__ void load_blk(int BL, const T *src, double *dst) {
     for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) dst[o] = (double)src[o];
@@ -75,18 +112,25 @@ __device__ __forceinline__ void store_blk(int BL, const double *src, T *dst) {
     for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) dst[o] = (T)src[o];
 }
 
-// In-place Gauss-Jordan inverse with partial pivoting (largest magnitude,
-// lowest index on ties, as LAPACK's idamax).  Returns false on a zero pivot.
-__device__ bool smem_inverse(int BL, double *A, int *piv, double *rowp, double *fcol, int *s_ok) {
+// Gauss-Jordan inverse with partial pivoting (largest magnitude, lowest
+// index on ties, as LAPACK's idamax), ping-ponging between two shared
+// buffers so that each elimination step costs two barriers: the row swap is
+// folded into the update (rows p and q trade places as they are read) and
+// the column swaps that undo the pivoting are composed into one permutation,
+// applied when the result is stored.  Every element sees the same operations
+// in the same order as the textbook in-place version.  Returns the buffer
+// that holds the result; column c of the inverse is its column perm[c].
+// *s_ok is cleared on a zero pivot.
+__device__ double *smem_inverse_db(int BL, double *A, double *B, int *piv, int *perm, int *s_ok) {
     if (threadIdx.x == 0) *s_ok = 1;
-    __syncthreads();
+    double *src = A, *dst = B;
     for (int p = 0; p < BL; p++) {
         if (threadIdx.x < 32) {
             const int lane = threadIdx.x;
             double best = -1.0;
             int bi = p;
             for (int r = p + lane; r < BL; r += 32) {
-                const double a = fabs(A[p * BL + r]);
+                const double a = fabs(src[p * BL + r]);
                 if (a > best) {
                     best = a;
                     bi = r;
@@ -108,36 +152,33 @@ __device__ bool smem_inverse(int BL, double *A, int *piv, double *rowp, double *
         }
         __syncthreads();
         const int q = piv[p];
-        if (q != p)
-            for (int c = threadIdx.x; c < BL; c += blockDim.x) {
-                const double t = A[c * BL + p];
-                A[c * BL + p] = A[c * BL + q];
-                A[c * BL + q] = t;
-            }
-        __syncthreads();
-        const double pv = A[p * BL + p];
+        const double pv = src[p * BL + q];
         const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
-        for (int c = threadIdx.x; c < BL; c += blockDim.x) rowp[c] = (c == p ? 1.0 : A[c * BL + p]) * inv;
-        for (int r = threadIdx.x; r < BL; r += blockDim.x) fcol[r] = (r == p) ? 0.0 : A[p * BL + r];
-        __syncthreads();
         for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) {
             const int r = o % BL, c = o / BL;
-            if (r == p) A[o] = rowp[c];
-            else A[o] = (c == p ? 0.0 : A[o]) - fcol[r] * rowp[c];
+            const double rp = (c == p ? 1.0 : src[c * BL + q]) * inv;  // pivot row, scaled
+            if (r == p) {
+                dst[o] = rp;
+            } else {
+                const int rs = (r == q) ? p : r;  // source row after the swap
+                dst[o] = (c == p ? 0.0 : src[c * BL + rs]) - src[p * BL + rs] * rp;
+            }
         }
         __syncthreads();
+        double *t = src;
+        src = dst;
+        dst = t;
     }
-    for (int p = BL - 1; p >= 0; p--) {
-        const int q = piv[p];
-        if (q != p)
-            for (int r = threadIdx.x; r < BL; r += blockDim.x) {
-                const double t = A[p * BL + r];
-                A[p * BL + r] = A[q * BL + r];
-                A[q * BL + r] = t;
-            }
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int c = 0; c < BL; c++) perm[c] = c;
+        for (int p = BL - 1; p >= 0; p--) {
+            const int q = piv[p], t = perm[p];
+            perm[p] = perm[q];
+            perm[q] = t;
+        }
     }
-    return *s_ok != 0;
+    __syncthreads();
+    return src;
 }
 
 constexpr int FT = 256;  // threads per factor CTA
@@ -158,8 +199,7 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict
     __shared__ int s_ok;
     const size_t b2 = (size_t)BL * BL;
     double *Ah = sm, *D = sm + b2, *X = sm + 2 * b2, *Y = sm + 3 * b2, *T = sm + 4 * b2;
-    double *rowp = sm + 5 * b2, *fcol = rowp + BL;
-    int *piv = (int *)(fcol + BL);
+    int *piv = (int *)(sm + 5 * b2), *perm = piv + BL;
     const int j = rows ? rows[blockIdx.x] : blockIdx.x;
     load_blk(BL, A + (size_t)diag_a[j] * b2, Ah);
     for (int p = lp_ptr[j]; p < lp_ptr[j + 1]; p++) {
@@ -167,31 +207,36 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict
         load_blk(BL, A + (size_t)lp_aji[p] * b2, X);
         load_blk(BL, A + (size_t)lp_aij[p] * b2, Y);
         __syncthreads();
-        smem_gemm(BL, X, D, T, false);  // L_ji
+        block_gemm(BL, X, D, T, false);  // L_ji
         __syncthreads();
         store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
-        smem_gemm(BL, T, Y, Ah, true);   // Ahat_jj -= L_ji A_ij
-        smem_gemm(BL, D, Y, X, false);   // U_ij
+        block_gemm(BL, T, Y, Ah, true);   // Ahat_jj -= L_ji A_ij
+        block_gemm(BL, D, Y, X, false);   // U_ij
         __syncthreads();
         store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
         __syncthreads();
     }
     __syncthreads();
-    const bool ok = smem_inverse(BL, Ah, piv, rowp, fcol, &s_ok);
-    if (!ok && threadIdx.x == 0) {
+    const double *Di = smem_inverse_db(BL, Ah, T, piv, perm, &s_ok);
+    if (!s_ok && threadIdx.x == 0) {
         atomicExch(flag, 1);
         atomicMin(flag + 1, j);
     }
     double *dj = dinv + (size_t)dinv_idx[j] * b2;
     TS *uj = Uv + (size_t)U_rowptr[j] * b2;
-    store_blk(BL, Ah, dj);
-    if ((void *)uj != (void *)dj) store_blk(BL, Ah, uj);
+    const bool both = (void *)uj != (void *)dj;
+    for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) {
+        const int r = o % BL, c = o / BL;
+        const double v = Di[perm[c] * BL + r];
+        dj[o] = v;
+        if (both) uj[o] = (TS)v;
+    }
 }
 
 template <class TA, class TS>
 cpg_status launch_factor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
     const int BL = P->bl;
-    const size_t smem = (5 * (size_t)BL * BL + 2 * BL) * sizeof(double) + BL * sizeof(int) + 16;
+    const size_t smem = 5 * (size_t)BL * BL * sizeof(double) + 2 * BL * sizeof(int) + 16;
     if ((int)smem > 48 * 1024)  // per launch: contexts on several host threads may share the kernel
         CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
@@ -213,11 +258,56 @@ cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrow
 void free_precond(cpg_precond *P) {
     void *ptrs[] = {P->lrows_d, P->urows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, P->U_rowptr_d, P->U_col_d,
                     P->U_vals, P->dinv64, P->dinv_idx_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d,
-                    P->lp_l_d, P->lp_u_d, P->diag_a_d};
+                    P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d};
     for (void *p : ptrs) dfree(p);
 }
 
 }  // namespace
+
+namespace cpg {
+
+cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+    if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
+    if (P->syncfree) {
+        // status word: flag_dev[2] = a wait ran out, flag_dev[4] = row counter
+        int *err = ctx->flag_dev + 2, *counter = ctx->flag_dev + 4;
+        const int g = ++P->generation;
+        CPG_TRY(sweep_op(ctx, P->precision, P->bl, P->n, P->lrows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, x,
+                         MODE_FORWARD, P->row_flags_d, 2 * g - 1, counter, err));
+        return sweep_op(ctx, P->precision, P->bl, P->n, P->urows_d, P->U_rowptr_d, P->U_col_d, P->U_vals, x,
+                        MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err);
+    }
+    if (P->kind == CPG_PC_ILU0) {
+        const int nl = (int)P->lptr.size() - 1;
+        for (int l = 0; l < nl; l++) {
+            const int cnt = P->lptr[l + 1] - P->lptr[l];
+            // rows without lower blocks pass through the forward sweep unchanged
+            CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->lrows_d + P->lptr[l], P->L_rowptr_d, P->L_col_d,
+                            P->L_vals, x, x, MODE_FORWARD));
+        }
+    }
+    const int nu = (int)P->uptr.size() - 1;
+    for (int l = 0; l < nu; l++) {
+        const int cnt = P->uptr[l + 1] - P->uptr[l];
+        CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->urows_d + P->uptr[l], P->U_rowptr_d, P->U_col_d,
+                        P->U_vals, x, x, MODE_BACKWARD));
+    }
+    return CPG_OK;
+}
+
+cpg_status check_sweep_error(cpg_ctx *ctx, cpg_status st) {
+    if (st != CPG_OK && st != CPG_ERR_NONFINITE && st != CPG_ERR_NOT_CONVERGED) return st;
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, ctx->flag_dev + 2, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep status");
+    if (!err) return st;
+    e = cudaMemsetAsync(ctx->flag_dev + 2, 0, sizeof(int), ctx->stream);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "sweep status reset");
+    return fail(ctx, CPG_ERR_TIMEOUT, "a triangular sweep's bounded wait on a row ran out");
+}
+
+}  // namespace cpg
 
 extern "C" {
 
@@ -329,7 +419,17 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     }
     std::vector<int> dinv_idx(n);
     for (int i = 0; i < n; i++) dinv_idx[i] = precision == CPG_F64 ? P->U_rowptr[i] : i;
+    const char *sweep_env = std::getenv("CPG_ILU_SWEEP");
+    const bool level_sweeps = sweep_env && std::strcmp(sweep_env, "levels") == 0;
+    P->syncfree = ilu && sweep_supported(P->bl) && !level_sweeps;
     cpg_status st = CPG_OK;
+    if (P->syncfree) {
+        st = dmalloc(ctx, &P->row_flags_d, (size_t)n);
+        if (st == CPG_OK) {
+            cudaError_t e = cudaMemsetAsync(P->row_flags_d, 0, sizeof(int) * n, ctx->stream);
+            if (e != cudaSuccess) st = cuda_fail(ctx, e, "row flags");
+        }
+    }
     auto up = [&](int **dst, const std::vector<int> &src) {
         if (st == CPG_OK) st = upload(ctx, dst, src);
     };
@@ -385,23 +485,7 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A) 
 
 cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     if (!ctx || !x) return CPG_ERR_INVALID_ARG;
-    if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
-    if (P->kind == CPG_PC_ILU0) {
-        const int nl = (int)P->lptr.size() - 1;
-        for (int l = 0; l < nl; l++) {
-            const int cnt = P->lptr[l + 1] - P->lptr[l];
-            // rows without lower blocks pass through the forward sweep unchanged
-            CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->lrows_d + P->lptr[l], P->L_rowptr_d, P->L_col_d,
-                            P->L_vals, x, x, MODE_FORWARD));
-        }
-    }
-    const int nu = (int)P->uptr.size() - 1;
-    for (int l = 0; l < nu; l++) {
-        const int cnt = P->uptr[l + 1] - P->uptr[l];
-        CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->urows_d + P->uptr[l], P->U_rowptr_d, P->U_col_d,
-                        P->U_vals, x, x, MODE_BACKWARD));
-    }
-    return CPG_OK;
+    return check_sweep_error(ctx, precond_apply_raw(ctx, P, x));
 }
 
 void cpg_precond_destroy(cpg_precond *P) {

@@ -312,7 +312,7 @@ struct StageOp : LinOp {
         const int64_t NS = S->N * s;
         k_stage_perm<<<grid_for(ctx, NS), 256, 0, ctx->stream>>>(n, s, bl, x, S->big2, 1);
         CPG_TRY(launched(ctx, "stage permute kernel"));
-        CPG_TRY(cpg_precond_apply(ctx, S->P, S->big2));
+        CPG_TRY(precond_apply_raw(ctx, S->P, S->big2));
         k_stage_perm<<<grid_for(ctx, NS), 256, 0, ctx->stream>>>(n, s, bl, S->big2, x, 0);
         return launched(ctx, "stage permute kernel");
     }
@@ -488,8 +488,12 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
         st->last_newton_residual = rNorm;
         if (rNorm < S->d.newton_tol) break;
         st->newton_iterations++;
+        // modified Newton: with reuse_jacobian = r > 0 the stage Jacobians,
+        // the coupled matrix and its factorisation are rebuilt every r-th
+        // iteration only (the reference rebuilds every iteration)
+        const bool rebuild = S->d.reuse_jacobian <= 0 || iter == 0 || iter % S->d.reuse_jacobian == 0;
         // stage Jacobians at the stage states
-        for (int i = 0; i < s; i++) {
+        for (int i = 0; i < s && rebuild; i++) {
             if (inv) CPG_TRY(combine(S, u, {{K + i * N, 1.0}}, S->cu));
             else {
                 Comb cb{};
@@ -504,7 +508,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
             CPG_TRY(cpg_jacobian(ctx, S->eq, S->cu, t + dt * S->c[i], 1.0, 0, S->Jview[i]));
         }
         cpg_solve_stats ls{};
-        if (kron) {
+        if (kron && rebuild) {
             const int grid = S->eq->n;
             const int64_t nnzb = (int64_t)S->eq->colidx.size();
             if (S->d.matrix_precision == CPG_F32)
@@ -518,12 +522,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
             CPG_TRY(launched(ctx, "stage block kernel"));
             if (S->P) CPG_TRY(cpg_precond_refactor(ctx, S->P, S->stage_blocks));
             else CPG_TRY(cpg_precond_create(ctx, S->stage_blocks, CPG_PC_BJACOBI, S->d.matrix_precision, &S->P));
-            StageOp op;
-            op.S = S;
-            op.dt = dt;
-            CPG_TRY(gmres_op(ctx, op, N * s, R, sol, S->d.gmres_m, S->d.gmres_tol, S->d.gmres_maxit, S->d.flexible,
-                             &ls));
-        } else {
+        } else if (!kron && rebuild) {
             CPG_TRY(fill_coupled(S, S->full, S->map_src, S->map_mrow, S->map_s1, S->map_s2, S->map_mc, dt));
             cpg_bsr *pcm = S->full;
             if (inv) {
@@ -532,6 +531,14 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
             }
             if (S->P) CPG_TRY(cpg_precond_refactor(ctx, S->P, pcm));
             else CPG_TRY(cpg_precond_create(ctx, pcm, S->d.pc_kind, S->d.matrix_precision, &S->P));
+        }
+        if (kron) {
+            StageOp op;
+            op.S = S;
+            op.dt = dt;
+            CPG_TRY(gmres_op(ctx, op, N * s, R, sol, S->d.gmres_m, S->d.gmres_tol, S->d.gmres_maxit, S->d.flexible,
+                             &ls));
+        } else {
             CPG_TRY(cpg_gmres(ctx, S->full, S->P, R, sol, S->d.gmres_m, S->d.gmres_tol, S->d.gmres_maxit,
                               S->d.flexible, &ls));
         }
