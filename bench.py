@@ -42,9 +42,17 @@ def parse():
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="dirk3", choices=["dirk3", "irk"],
+    ap.add_argument("--workload", default="dirk3", choices=["dirk3", "irk", "serve"],
                     help="dirk3: the 100k-cell vortex (default); irk: 2-stage Radau IIA, 500k cells, walls/inflow/"
-                         "outflow, stage block-Jacobi GMRES(40) 1e-9")
+                         "outflow, stage block-Jacobi GMRES(40) 1e-9; serve: Poisson stream of independent solves")
+    ap.add_argument("--newton-tol", type=float, default=5e-13,
+                    help="Newton tolerance on the residual's L2 norm (reference: 5e-13)")
+    ap.add_argument("--reuse-jacobian", type=int, default=0,
+                    help="rebuild the Jacobian and preconditioner every k-th Newton iteration (0 = every one)")
+    ap.add_argument("--requests", type=int, default=512, help="serve: requests in the timed stream")
+    ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate, requests/s")
+    ap.add_argument("--slots", type=int, default=8, help="serve: requests in flight at most")
+    ap.add_argument("--max-seeds", type=int, default=50000, help="serve: largest mesh of the stream")
     ap.add_argument("--compare-fp64", type=int, default=0,
                     help="with --precision mixed: steps over which to measure the error against the FP64 path")
     a = ap.parse_args()
@@ -60,19 +68,27 @@ def parse():
 
 def workload(a) -> dict:
     prec = 'FP32 blocks + FGMRES' if a.precision == 'mixed' else 'FP64'
+    if a.workload == "serve":
+        return {"workload": f"serving stream: {a.requests} independent solves, Poisson arrivals at {a.rate}/s; 50% "
+                            f"advection (p in 1..3, random angle), 50% Euler vortex (p in 2..3, strength 1..5); "
+                            f"Voronoi meshes of 500-{a.max_seeds} seeds (log-uniform); RK4 or DIRK3 (GMRES(30) + "
+                            f"ILU(0) 1e-10), 10-100 steps; admission by HBM footprint, {a.slots} slots",
+                "requests": a.requests, "rate": a.rate, "slots": a.slots, "max_seeds": a.max_seeds,
+                "l2": "each request streams its own state; no L2 flush"}
     if a.workload == "irk":
         return {"workload": f"euler-density-bump Mach 0.3, [0,10]^2 slip walls / inflow / outflow, {a.cells} Voronoi "
                             f"cells (seed 5), p={a.degree}, 2-stage Radau IIA dt={a.dt}, GMRES(40) + block Jacobi on "
-                            f"48x48 cell-coupled stage blocks tol 1e-9, Newton 5e-13, {prec}",
+                            f"48x48 cell-coupled stage blocks tol 1e-9, Newton {a.newton_tol:g}, {prec}",
                 "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
                 "dt": a.dt, "gmres_m": 40, "gmres_tol": 1e-9, "preconditioner": "stage block Jacobi",
-                "precision": a.precision, "jacobian": "exact",
+                "precision": a.precision, "jacobian": "exact", "newton_tol": a.newton_tol,
+                "reuse_jacobian": a.reuse_jacobian,
                 "l2": "inputs larger than L2: each stage Jacobian streams ~16 GB per matvec"}
     return {"workload": f"euler-isentropic-vortex periodic [0,10]^2, {a.cells} Voronoi cells (seed 2), p={a.degree}, "
-                        f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton 5e-13, {prec}",
+                        f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton {a.newton_tol:g}, {prec}",
             "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
             "dt": a.dt, "gmres_m": 30, "gmres_tol": 1e-10, "preconditioner": "ilu0",
-            "precision": a.precision,
+            "precision": a.precision, "newton_tol": a.newton_tol, "reuse_jacobian": a.reuse_jacobian,
             "jacobian": "exact (the reference's A_x entry and own-state neighbour blocks corrected; same residual "
                         "and converged solution, quadratic Newton); the CPU arm runs the reference's Jacobian",
             "l2": "inputs larger than L2: the Jacobian and ILU factors stream ~9 GB each per sweep"}
@@ -192,6 +208,10 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if a.workload == "serve":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; its per-solve "
+                          "CPU cost is measured by the dirk3 and irk workloads"}), flush=True)
+        return
     vals = []
     info = None
     for k in range(a.warmup + a.steps):
@@ -228,7 +248,8 @@ def build_problem(a, cp, ctx):
 
         def make(mixed):
             return cp.IRK(2, eq, pc=cp.PC_STAGE_BJACOBI, precision=cp.F32 if mixed else cp.F64, gmres_m=40,
-                          gmres_tol=1e-9, gmres_maxit=20000, flexible=mixed)
+                          gmres_tol=1e-9, gmres_maxit=20000, flexible=mixed, newton_tol=a.newton_tol,
+                          reuse_jacobian=a.reuse_jacobian)
         return eq, make, u0
     seeds = cp.uniform_seeds(2, a.cells, WIDTH, WIDTH)
     mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
@@ -237,11 +258,78 @@ def build_problem(a, cp, ctx):
 
     def make(mixed):
         return cp.DIRK(3, eq, pc=cp.PC_ILU0, precision=cp.F32 if mixed else cp.F64, gmres_m=30, gmres_tol=1e-10,
-                       gmres_maxit=90000, flexible=mixed)
+                       gmres_maxit=90000, flexible=mixed, newton_tol=a.newton_tol,
+                       reuse_jacobian=a.reuse_jacobian)
     return eq, make, u0
 
 
 # ------------------------------------------------------------------ GPU arm
+def replica_throughput(local_ms: float, units: int, world: int, dist=None, device=None):
+    """Replicas: every rank processes `units` on its own device; the job
+    time is the slowest rank's device time.  Returns (max ms, units/s of the
+    whole job)."""
+    import torch
+    if dist is not None and world > 1:
+        dev = device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu")
+        t = torch.tensor([local_ms], dtype=torch.float64, device=dev)
+        dist.barrier()
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        local_ms = float(t.item())
+    return local_ms, world * units / (local_ms / 1000.0)
+
+
+def run_serve(a):
+    """Serving stream through cpolyg_b200.serve.Server: solves/s over the
+    stream's makespan, p50/p99 latency from arrival to result on the host."""
+    import torch
+
+    from cpolyg_b200 import serve
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
+    # warm-up: a few small requests (library load, first-use kernel tuning)
+    warm = serve.make_stream(max(a.warmup, 3), rate=1e6, seed=10_000 + rank, max_seeds=3000, max_steps=12)
+    serve.Server(slots=a.slots, device=local).serve(warm, realtime=False)
+    stream = serve.make_stream(a.requests, rate=a.rate, seed=rank, max_seeds=a.max_seeds)
+    srv = serve.Server(slots=a.slots, device=local)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    stats = srv.serve(stream, realtime=True)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms_max, value = replica_throughput(stats["makespan_s"] * 1e3, stats["solves"], world, dist, f"cuda:{local}")
+    if rank == 0:
+        h2d = sum(r.n_seeds * 16 for r in stream)  # seeds go to the device as part of each request
+        d2h = sum(r.result.nbytes for r in stream if r.result is not None)
+        out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.requests,
+               "warmup": len(warm), "ms_per_step": ms_max / max(1, stats["solves"]), "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+               "data": "synthetic (seeded Voronoi meshes, analytic initial data, Poisson arrivals)",
+               "config": dict(workload(a), parallelism=f"replicas x{world}"),
+               "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "failed": stats["failed"],
+               "peak_in_flight": stats["peak_in_flight"], "peak_bytes": stats["peak_bytes"],
+               "newton_iterations": sum(r.newton for r in stream), "gmres_iterations": sum(r.gmres for r in stream),
+               "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": h2d // max(1, a.requests),
+                       "d2h_bytes_per_step": d2h // max(1, a.requests),
+                       "note": "the serving loop is end to end: host seeds in, host coefficients out"},
+               "clocks": clk}
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -305,12 +393,7 @@ def run_ours(a):
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launches - launches0
     clk = clocks.stop()
-    ms_t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.barrier()
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
-    value = world * a.steps / (ms_max / 1000.0)
+    ms_max, value = replica_throughput(ms, a.steps, world, dist)
 
     # end to end through the C ABI with host buffers (cpg_step_host)
     e2e = None
@@ -392,6 +475,8 @@ def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.workload == "serve":
+        run_serve(a)
     else:
         run_ours(a)
 

@@ -365,10 +365,11 @@ bool tunable(int bl) { return bl == 6 || bl == 10 || bl == 24 || bl == 40 || bl 
 int tuned_variant(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rowptr, const int *col,
                   const void *vals, const double *x, double *y) {
     if (!tunable(bl)) return 0;
-    {
-        std::lock_guard<std::mutex> lk(g_tune_mu);
-        if (g_tune[precision][bl]) return g_tune[precision][bl] - 1;
-    }
+    // held for the whole tuning: concurrent first calls (serving threads)
+    // wait and then read the one decision, so every solve of the process
+    // uses the same variant and sums in the same order
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune[precision][bl]) return g_tune[precision][bl] - 1;
     const char *env = std::getenv("CPG_AUTOTUNE");
     if ((env && std::strcmp(env, "0") == 0) || nrows < 2048) return 0;
     cudaEvent_t e0, e1;
@@ -396,7 +397,6 @@ int tuned_variant(cpg_ctx *ctx, int precision, int bl, int nrows, const int *row
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    std::lock_guard<std::mutex> lk(g_tune_mu);
     g_tune[precision][bl] = best + 1;
     return best;
 }
