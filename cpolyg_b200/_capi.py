@@ -105,6 +105,8 @@ PROTOTYPES = {
     "cpg_precond_create": (I, [P, P, I, I, PP]),
     "cpg_precond_refactor": (I, [P, P, P]),
     "cpg_precond_apply": (I, [P, P, P]),
+    "cpg_precond_sweep_form": (I, [P]),
+    "cpg_debug_sweep_timeout": (I, [P]),
     "cpg_precond_destroy": (None, [P]),
     "cpg_precond_levels": (I, [P, PI, PI, PI, PI, PI, PI]),
     "cpg_precond_export": (I, [P, P, PD, PI, PI, PD, PI, PI, PD]),

@@ -189,8 +189,10 @@ __global__ void __launch_bounds__(TPR) k_sweep(const int *__restrict__ order, in
                                                int mode, int *flags, int gen, int *counter, int *err) {
     static_assert((TPR * VEC) % BL == 0, "stride must be a multiple of the block size");
     static_assert(BL % VEC == 0, "vector width must divide the block size");
+    static_assert(TPR >= 64, "the claiming thread lives in the second warp");
     constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
-    __shared__ int s_row;
+    constexpr int CLAIMER = 32;  // warp 0 holds the dependency waits
+    __shared__ int s_row[2];
     __shared__ int scol[MAX_ROW_BLOCKS];
     __shared__ double red[G][BL];
     const int tid = threadIdx.x;
@@ -198,11 +200,13 @@ __global__ void __launch_bounds__(TPR) k_sweep(const int *__restrict__ order, in
     const int r0 = e0 % BL, g = e0 / BL;
     const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
     const double sr = -1.0;
-    for (;;) {
-        if (tid == 0) s_row = atomicAdd(counter, 1);
-        __syncthreads();
-        const int q = s_row;
+    if (tid == CLAIMER) s_row[0] = atomicAdd(counter, 1);
+    __syncthreads();
+    for (int cur = 0;; cur ^= 1) {
+        const int q = s_row[cur];
         if (q >= n) break;
+        // claim the next row now, so the atomic's round trip hides behind this row
+        if (tid == CLAIMER) s_row[cur ^ 1] = atomicAdd(counter, 1);
         const int i = order[q];
         const int k0 = rowptr[i], nblk = rowptr[i + 1] - k0;
         // the backward row's first block is D^{-1}_i (its own column)
@@ -255,10 +259,12 @@ __global__ void __launch_bounds__(TPR) k_sweep(const int *__restrict__ order, in
             double *xi = x + (size_t)i * BL;
             if (mode == MODE_FORWARD) s = __ldcg(xi + tid) + s;
             __stcg(xi + tid, s);
-            __threadfence();
         }
-        __syncthreads();
-        if (tid == 0) st_release(flags + i, gen);
+        __syncthreads();  // the row's stores (and the next claim) are done
+        if (tid == 0) {
+            __threadfence();
+            st_release(flags + i, gen);
+        }
     }
 }
 

@@ -91,6 +91,13 @@ struct cpg_precond {
     bool syncfree = false;
     int *row_flags_d = nullptr;
     mutable int generation = 0;
+    // sweep form when both are possible (results are bitwise identical):
+    // 0 = still timing (applications alternate between the forms), 1 =
+    // sync-free, 2 = level sweeps
+    mutable int sweep_mode = 0;
+    mutable int tune_count = 0, tune_pending = -1;
+    mutable float tune_ms[2] = {1e30f, 1e30f};
+    mutable cudaEvent_t tune_ev[2] = {nullptr, nullptr};
     int64_t nnzL = 0, nnzU = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
 };

@@ -112,56 +112,57 @@ __device__ __forceinline__ void store_blk(int BL, const double *src, T *dst) {
     for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) dst[o] = (T)src[o];
 }
 
-// Gauss-Jordan inverse with partial pivoting (largest magnitude, lowest
-// index on ties, as LAPACK's idamax), ping-ponging between two shared
-// buffers so that each elimination step costs two barriers: the row swap is
-// folded into the update (rows p and q trade places as they are read) and
-// the column swaps that undo the pivoting are composed into one permutation,
-// applied when the result is stored.  Every element sees the same operations
-// in the same order as the textbook in-place version.  Returns the buffer
-// that holds the result; column c of the inverse is its column perm[c].
-// *s_ok is cleared on a zero pivot.
-__device__ double *smem_inverse_db(int BL, double *A, double *B, int *piv, int *perm, int *s_ok) {
-    if (threadIdx.x == 0) *s_ok = 1;
+constexpr int FT = 320;  // threads per factor CTA: 8 columns x 40 rows of a 40x40 block at a time
+
+// Gauss-Jordan inverse with partial pivoting and one barrier per elimination
+// step.  Every warp finds the pivot of column p by itself (the same reads and
+// the same tie-break, so all warps agree), which removes the barrier a
+// single pivot-searching warp would need.  Each thread owns one row r and
+// the columns cfirst, cfirst + cstep, ...; the row swap is folded into the
+// reads (rows p and q trade places) and the update ping-pongs between two
+// buffers.  Every element sees the same operations in the same order as the
+// textbook in-place version (pivot: largest magnitude, lowest index on ties,
+// as LAPACK's idamax).  The column swaps that undo the pivoting are composed
+// into perm: column c of the inverse is column perm[c] of the returned
+// buffer.  *s_ok is cleared on a zero pivot.
+__device__ __forceinline__ double *smem_inverse(int BL, double *A, double *B, int *piv, int *perm, int *s_ok) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int cstep = FT / BL, r = tid % BL, cfirst = tid / BL;
+    const bool owner = cfirst < cstep;
+    if (tid == 0) *s_ok = 1;
     double *src = A, *dst = B;
     for (int p = 0; p < BL; p++) {
-        if (threadIdx.x < 32) {
-            const int lane = threadIdx.x;
-            double best = -1.0;
-            int bi = p;
-            for (int r = p + lane; r < BL; r += 32) {
-                const double a = fabs(src[p * BL + r]);
-                if (a > best) {
-                    best = a;
-                    bi = r;
-                }
-            }
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) {
-                const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-                const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                if (ob > best || (ob == best && oi < bi)) {
-                    best = ob;
-                    bi = oi;
-                }
-            }
-            if (lane == 0) {
-                piv[p] = bi;
-                if (!(best > 0.0)) *s_ok = 0;
+        double best = -1.0;
+        int bi = p;
+        for (int rr = p + lane; rr < BL; rr += 32) {
+            const double a = fabs(src[p * BL + rr]);
+            if (a > best) {
+                best = a;
+                bi = rr;
             }
         }
-        __syncthreads();
-        const int q = piv[p];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+            if (ob > best || (ob == best && oi < bi)) {
+                best = ob;
+                bi = oi;
+            }
+        }
+        const int q = bi;
+        if (tid == 0) {
+            piv[p] = q;
+            if (!(best > 0.0)) *s_ok = 0;
+        }
         const double pv = src[p * BL + q];
         const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
-        for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) {
-            const int r = o % BL, c = o / BL;
-            const double rp = (c == p ? 1.0 : src[c * BL + q]) * inv;  // pivot row, scaled
-            if (r == p) {
-                dst[o] = rp;
-            } else {
-                const int rs = (r == q) ? p : r;  // source row after the swap
-                dst[o] = (c == p ? 0.0 : src[c * BL + rs]) - src[p * BL + rs] * rp;
+        if (owner) {
+            const int rs = (r == q) ? p : r;  // source row after the swap
+            const double f = src[p * BL + rs];
+            for (int c = cfirst; c < BL; c += cstep) {
+                const double rp = (c == p ? 1.0 : src[c * BL + q]) * inv;  // pivot row, scaled
+                dst[c * BL + r] = (r == p) ? rp : (c == p ? 0.0 : src[c * BL + rs]) - f * rp;
             }
         }
         __syncthreads();
@@ -169,7 +170,7 @@ __device__ double *smem_inverse_db(int BL, double *A, double *B, int *piv, int *
         src = dst;
         dst = t;
     }
-    if (threadIdx.x == 0) {
+    if (tid == 0) {
         for (int c = 0; c < BL; c++) perm[c] = c;
         for (int p = BL - 1; p >= 0; p--) {
             const int q = piv[p], t = perm[p];
@@ -181,14 +182,52 @@ __device__ double *smem_inverse_db(int BL, double *A, double *B, int *piv, int *
     return src;
 }
 
-constexpr int FT = 256;  // threads per factor CTA
+// Product whose output goes straight from the DMMA fragments to global
+// memory (no shared-memory round trip): C = A * B, BL % 8 == 0.
+template <class T>
+__device__ __forceinline__ void dmma_gemm_to_global(int BL, const double *A, const double *B, T *C) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int nt = BL >> 3;
+    for (int tile = warp; tile < nt * nt; tile += nw) {
+        const int r0 = (tile % nt) * 8, c0 = (tile / nt) * 8;
+        double d0 = 0.0, d1 = 0.0;
+        for (int k = 0; k < BL; k += 4)
+            dmma_m8n8k4(d0, d1, A[(k + t) * BL + r0 + g], B[(c0 + g) * BL + k + t]);
+        T *cc = C + (size_t)(c0 + 2 * t) * BL + r0 + g;
+        cc[0] = (T)d0;
+        cc[BL] = (T)d1;
+    }
+}
+
+// block -> registers (PER elements per thread, element o = tid + k*FT)
+template <int PER, class T>
+__device__ __forceinline__ void fetch_blk(int BL2, const T *src, double (&v)[PER]) {
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const int o = threadIdx.x + k * FT;
+        v[k] = o < BL2 ? (double)src[o] : 0.0;
+    }
+}
+template <int PER>
+__device__ __forceinline__ void stash_blk(int BL2, const double (&v)[PER], double *dst) {
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const int o = threadIdx.x + k * FT;
+        if (o < BL2) dst[o] = v[k];
+    }
+}
 
 // One CTA per row j of the level:
 //   for each lower neighbour i < j (ascending):
 //       L_ji = A_ji D_i^{-1}; Ahat_jj -= L_ji A_ij; U_ij = D_i^{-1} A_ij
 //   D_j^{-1} = inv(Ahat_jj)
-template <class TA, class TS>
-__global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict__ rows, const TA *__restrict__ A,
+// BLC > 0 compiles the block size in: the three blocks of the next lower
+// neighbour are then fetched into registers while the current products run,
+// and with BLC % 8 == 0 the products run on DMMA with U_ij stored straight
+// from the fragments.  BLC == 0 is the generic path (any block size).
+template <class TA, class TS, int BLC>
+__global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restrict__ rows, const TA *__restrict__ A,
                                                    const int *__restrict__ diag_a, const int *__restrict__ lp_ptr,
                                                    const int *__restrict__ lp_i, const int *__restrict__ lp_aji,
                                                    const int *__restrict__ lp_aij, const int *__restrict__ lp_l,
@@ -197,27 +236,69 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict
                                                    double *dinv, const int *__restrict__ dinv_idx, int *flag) {
     extern __shared__ double sm[];
     __shared__ int s_ok;
-    const size_t b2 = (size_t)BL * BL;
+    const int BL = BLC ? BLC : bl_rt;
+    const int BL2 = BL * BL;
+    const size_t b2 = (size_t)BL2;
     double *Ah = sm, *D = sm + b2, *X = sm + 2 * b2, *Y = sm + 3 * b2, *T = sm + 4 * b2;
     int *piv = (int *)(sm + 5 * b2), *perm = piv + BL;
     const int j = rows ? rows[blockIdx.x] : blockIdx.x;
-    load_blk(BL, A + (size_t)diag_a[j] * b2, Ah);
-    for (int p = lp_ptr[j]; p < lp_ptr[j + 1]; p++) {
-        load_blk(BL, dinv + (size_t)dinv_idx[lp_i[p]] * b2, D);
-        load_blk(BL, A + (size_t)lp_aji[p] * b2, X);
-        load_blk(BL, A + (size_t)lp_aij[p] * b2, Y);
-        __syncthreads();
-        block_gemm(BL, X, D, T, false);  // L_ji
-        __syncthreads();
-        store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
-        block_gemm(BL, T, Y, Ah, true);   // Ahat_jj -= L_ji A_ij
-        block_gemm(BL, D, Y, X, false);   // U_ij
-        __syncthreads();
-        store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
-        __syncthreads();
+    const int p0 = lp_ptr[j], p1 = lp_ptr[j + 1];
+    if constexpr (BLC > 0) {
+        constexpr int PER = (BLC * BLC + FT - 1) / FT;
+        constexpr bool TC = (BLC % 8) == 0;
+        double rd[PER], rx[PER], ry[PER];
+        if (p0 < p1) {
+            fetch_blk<PER>(BL2, dinv + (size_t)dinv_idx[lp_i[p0]] * b2, rd);
+            fetch_blk<PER>(BL2, A + (size_t)lp_aji[p0] * b2, rx);
+            fetch_blk<PER>(BL2, A + (size_t)lp_aij[p0] * b2, ry);
+        }
+        load_blk(BL, A + (size_t)diag_a[j] * b2, Ah);
+        for (int p = p0; p < p1; p++) {
+            stash_blk<PER>(BL2, rd, D);
+            stash_blk<PER>(BL2, rx, X);
+            stash_blk<PER>(BL2, ry, Y);
+            __syncthreads();
+            if (p + 1 < p1) {  // next neighbour's blocks in flight during the products
+                fetch_blk<PER>(BL2, dinv + (size_t)dinv_idx[lp_i[p + 1]] * b2, rd);
+                fetch_blk<PER>(BL2, A + (size_t)lp_aji[p + 1] * b2, rx);
+                fetch_blk<PER>(BL2, A + (size_t)lp_aij[p + 1] * b2, ry);
+            }
+            if constexpr (TC) {
+                smem_gemm_dmma(BL, X, D, T, false);                           // L_ji
+                dmma_gemm_to_global(BL, D, Y, Uv + (size_t)lp_u[p] * b2);     // U_ij
+                __syncthreads();
+                store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
+                smem_gemm_dmma(BL, T, Y, Ah, true);                           // Ahat_jj -= L_ji A_ij
+            } else {
+                smem_gemm(BL, X, D, T, false);
+                __syncthreads();
+                store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
+                smem_gemm(BL, T, Y, Ah, true);
+                smem_gemm(BL, D, Y, X, false);
+                __syncthreads();
+                store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
+            }
+            __syncthreads();
+        }
+    } else {
+        load_blk(BL, A + (size_t)diag_a[j] * b2, Ah);
+        for (int p = p0; p < p1; p++) {
+            load_blk(BL, dinv + (size_t)dinv_idx[lp_i[p]] * b2, D);
+            load_blk(BL, A + (size_t)lp_aji[p] * b2, X);
+            load_blk(BL, A + (size_t)lp_aij[p] * b2, Y);
+            __syncthreads();
+            block_gemm(BL, X, D, T, false);  // L_ji
+            __syncthreads();
+            store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
+            block_gemm(BL, T, Y, Ah, true);   // Ahat_jj -= L_ji A_ij
+            block_gemm(BL, D, Y, X, false);   // U_ij
+            __syncthreads();
+            store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
+            __syncthreads();
+        }
     }
     __syncthreads();
-    const double *Di = smem_inverse_db(BL, Ah, T, piv, perm, &s_ok);
+    const double *Di = smem_inverse(BL, Ah, T, piv, perm, &s_ok);
     if (!s_ok && threadIdx.x == 0) {
         atomicExch(flag, 1);
         atomicMin(flag + 1, j);
@@ -225,7 +306,7 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict
     double *dj = dinv + (size_t)dinv_idx[j] * b2;
     TS *uj = Uv + (size_t)U_rowptr[j] * b2;
     const bool both = (void *)uj != (void *)dj;
-    for (int o = threadIdx.x; o < BL * BL; o += blockDim.x) {
+    for (int o = threadIdx.x; o < BL2; o += FT) {
         const int r = o % BL, c = o / BL;
         const double v = Di[perm[c] * BL + r];
         dj[o] = v;
@@ -233,18 +314,31 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int BL, const int *__restrict
     }
 }
 
-template <class TA, class TS>
-cpg_status launch_factor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
+template <class TA, class TS, int BLC>
+cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
     const int BL = P->bl;
     const size_t smem = 5 * (size_t)BL * BL * sizeof(double) + 2 * BL * sizeof(int) + 16;
     if ((int)smem > 48 * 1024)  // per launch: contexts on several host threads may share the kernel
-        CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS, BLC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
     double *dinv = P->precision == CPG_F64 ? (double *)P->U_vals : P->dinv64;
-    k_ilu_factor<TA, TS><<<nrows, FT, smem, ctx->stream>>>(
+    k_ilu_factor<TA, TS, BLC><<<nrows, FT, smem, ctx->stream>>>(
         BL, rows, (const TA *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
         P->lp_u_d, (TS *)P->L_vals, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
     return launched(ctx, "ilu factor kernel");
+}
+
+template <class TA, class TS>
+cpg_status launch_factor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
+    if (P->bl > FT) return fail(ctx, CPG_ERR_UNSUPPORTED, "block size above the factor kernel's thread count");
+    switch (P->bl) {
+        case 6: return launch_factor_bl<TA, TS, 6>(ctx, P, A, nrows, rows);
+        case 10: return launch_factor_bl<TA, TS, 10>(ctx, P, A, nrows, rows);
+        case 24: return launch_factor_bl<TA, TS, 24>(ctx, P, A, nrows, rows);
+        case 40: return launch_factor_bl<TA, TS, 40>(ctx, P, A, nrows, rows);
+        case 48: return launch_factor_bl<TA, TS, 48>(ctx, P, A, nrows, rows);
+        default: return launch_factor_bl<TA, TS, 0>(ctx, P, A, nrows, rows);
+    }
 }
 
 cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
@@ -255,28 +349,39 @@ cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrow
     return launch_factor<float, double>(ctx, P, A, nrows, rows);
 }
 
+void drop_tune_events(const cpg_precond *P) {
+    for (cudaEvent_t &e : P->tune_ev)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+}
+
 void free_precond(cpg_precond *P) {
     void *ptrs[] = {P->lrows_d, P->urows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, P->U_rowptr_d, P->U_col_d,
                     P->U_vals, P->dinv64, P->dinv_idx_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d,
                     P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d};
     for (void *p : ptrs) dfree(p);
+    drop_tune_events(P);
 }
 
 }  // namespace
 
 namespace cpg {
 
-cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x) {
-    if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
-    if (P->syncfree) {
-        // status word: flag_dev[2] = a wait ran out, flag_dev[4] = row counter
-        int *err = ctx->flag_dev + 2, *counter = ctx->flag_dev + 4;
-        const int g = ++P->generation;
-        CPG_TRY(sweep_op(ctx, P->precision, P->bl, P->n, P->lrows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, x,
-                         MODE_FORWARD, P->row_flags_d, 2 * g - 1, counter, err));
-        return sweep_op(ctx, P->precision, P->bl, P->n, P->urows_d, P->U_rowptr_d, P->U_col_d, P->U_vals, x,
-                        MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err);
-    }
+namespace sweep_form {
+
+cpg_status apply_syncfree(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+    // status word: flag_dev[2] = a wait ran out, flag_dev[4] = row counter
+    int *err = ctx->flag_dev + 2, *counter = ctx->flag_dev + 4;
+    const int g = ++P->generation;
+    CPG_TRY(sweep_op(ctx, P->precision, P->bl, P->n, P->lrows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, x,
+                     MODE_FORWARD, P->row_flags_d, 2 * g - 1, counter, err));
+    return sweep_op(ctx, P->precision, P->bl, P->n, P->urows_d, P->U_rowptr_d, P->U_col_d, P->U_vals, x,
+                    MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err);
+}
+
+cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     if (P->kind == CPG_PC_ILU0) {
         const int nl = (int)P->lptr.size() - 1;
         for (int l = 0; l < nl; l++) {
@@ -293,6 +398,45 @@ cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x) {
                         P->U_vals, x, x, MODE_BACKWARD));
     }
     return CPG_OK;
+}
+
+// Picks the faster sweep form on the preconditioner's own rows: the first
+// four applications alternate between the forms (each timed with events on
+// the stream), the fifth reads the timings and settles.  Both forms stream
+// the same rows with the same threads per row and sum in the same order, so
+// the results do not depend on the choice.
+cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+    if (P->tune_pending >= 0) {
+        float ms = 1e30f;
+        if (cudaEventSynchronize(P->tune_ev[1]) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, P->tune_ev[0], P->tune_ev[1]) == cudaSuccess)
+            P->tune_ms[P->tune_pending] = std::min(P->tune_ms[P->tune_pending], ms);
+        P->tune_pending = -1;
+    }
+    if (P->tune_count >= 4 || (!P->tune_ev[0] && (cudaEventCreate(&P->tune_ev[0]) != cudaSuccess ||
+                                                  cudaEventCreate(&P->tune_ev[1]) != cudaSuccess))) {
+        (void)cudaGetLastError();
+        P->sweep_mode = P->tune_ms[1] < P->tune_ms[0] ? 2 : 1;
+        drop_tune_events(P);
+        return P->sweep_mode == 1 ? apply_syncfree(ctx, P, x) : apply_levels(ctx, P, x);
+    }
+    const int which = P->tune_count++ % 2;
+    CPG_CUDA(ctx, cudaEventRecord(P->tune_ev[0], ctx->stream));
+    CPG_TRY(which == 0 ? apply_syncfree(ctx, P, x) : apply_levels(ctx, P, x));
+    CPG_CUDA(ctx, cudaEventRecord(P->tune_ev[1], ctx->stream));
+    P->tune_pending = which;
+    return CPG_OK;
+}
+
+}  // namespace sweep_form
+
+cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+    if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
+    if (P->syncfree) {
+        if (P->sweep_mode == 1) return sweep_form::apply_syncfree(ctx, P, x);
+        if (P->sweep_mode == 0) return sweep_form::apply_tuning(ctx, P, x);
+    }
+    return sweep_form::apply_levels(ctx, P, x);
 }
 
 cpg_status check_sweep_error(cpg_ctx *ctx, cpg_status st) {
@@ -422,6 +566,8 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     const char *sweep_env = std::getenv("CPG_ILU_SWEEP");
     const bool level_sweeps = sweep_env && std::strcmp(sweep_env, "levels") == 0;
     P->syncfree = ilu && sweep_supported(P->bl) && !level_sweeps;
+    // CPG_ILU_SWEEP=syncfree skips the timing of the two forms
+    if (sweep_env && std::strcmp(sweep_env, "syncfree") == 0) P->sweep_mode = 1;
     cpg_status st = CPG_OK;
     if (P->syncfree) {
         st = dmalloc(ctx, &P->row_flags_d, (size_t)n);
@@ -486,6 +632,39 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A) 
 cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     if (!ctx || !x) return CPG_ERR_INVALID_ARG;
     return check_sweep_error(ctx, precond_apply_raw(ctx, P, x));
+}
+
+int cpg_precond_sweep_form(const cpg_precond *P) {
+    if (!P || P->kind != CPG_PC_ILU0) return 0;
+    return P->syncfree ? P->sweep_mode : 2;
+}
+
+cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx) {
+    if (!ctx) return CPG_ERR_INVALID_ARG;
+    // rows 0 and 1 (6x6 blocks); row 1 reads row 0, but only row 1 is in the
+    // sweep's order, so row 0's flag is never published
+    const int h_rowptr[3] = {0, 0, 1}, h_col[1] = {0}, h_order[1] = {1};
+    int *ibuf = nullptr;
+    double *dbuf = nullptr;
+    CPG_TRY(dmalloc(ctx, &ibuf, 16));
+    cpg_status st = dmalloc(ctx, &dbuf, 36 + 12);
+    if (st == CPG_OK) {
+        int *rowptr = ibuf, *col = ibuf + 3, *order = ibuf + 4, *flags = ibuf + 5;
+        cudaError_t e = cudaMemsetAsync(ibuf, 0, 16 * sizeof(int), ctx->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(dbuf, 0, 48 * sizeof(double), ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rowptr, h_rowptr, sizeof(h_rowptr), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(col, h_col, sizeof(h_col), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(order, h_order, sizeof(h_order), cudaMemcpyHostToDevice, ctx->stream);
+        if (e != cudaSuccess) st = cuda_fail(ctx, e, "sweep check setup");
+        if (st == CPG_OK)
+            st = sweep_op(ctx, CPG_F64, 6, 1, order, rowptr, col, dbuf, dbuf + 36, MODE_FORWARD, flags, 1,
+                          ctx->flag_dev + 4, ctx->flag_dev + 2);
+        st = check_sweep_error(ctx, st);
+    }
+    cudaStreamSynchronize(ctx->stream);
+    dfree(ibuf);
+    dfree(dbuf);
+    return st;
 }
 
 void cpg_precond_destroy(cpg_precond *P) {

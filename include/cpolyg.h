@@ -296,6 +296,18 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A);
 /* Preconditioner::solve(double *x): x <- P^{-1} x in place                  */
 cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x_dev);
 void cpg_precond_destroy(cpg_precond *P);
+/* Triangular sweep form of an ILU(0) preconditioner: 1 = sync-free (one
+ * launch per sweep), 2 = one launch per level, 0 = not decided yet (the
+ * first four applications time both forms; both give bitwise-identical
+ * results).  CPG_ILU_SWEEP=levels or =syncfree in the environment when the
+ * preconditioner is created forces a form.  No counterpart in the reference
+ * (its sweeps are sequential loops, Preconditioners.cpp:125-158).           */
+int cpg_precond_sweep_form(const cpg_precond *P);
+/* Failure-detection check of the sync-free sweep: runs a one-row sweep whose
+ * dependency is never published, so the row's bounded wait runs out (well
+ * under ten seconds); returns CPG_ERR_TIMEOUT when the kernel reported it
+ * and leaves the context usable.  No counterpart in the reference.          */
+cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx);
 /* ILU(0) level schedule (row lists by level), for checks:
  *   lower_ptr[levels_lower+1], lower_rows[n], upper_ptr[...], upper_rows[n] */
 cpg_status cpg_precond_levels(const cpg_precond *P, int *n_lower,

@@ -117,7 +117,7 @@ def test_matvec(ctx, bl, prec):
     assert rel(y, ref) < (1e-13 if prec == cp.F64 else 1e-13)
 
 
-@pytest.mark.parametrize("bl", [3, 6, 10, 24, 40])
+@pytest.mark.parametrize("bl", [3, 6, 10, 12, 16, 24, 40, 48])
 def test_ilu0_factor_apply_and_levels(ctx, bl):
     rp, cl, blocks = random_bsr(60, bl, seed=5)
     A = cp.BlockMatrix.from_host(ctx, rp, cl, blocks)

@@ -1,0 +1,68 @@
+"""Triangular sweep forms of the block ILU(0) preconditioner.
+
+The sync-free form (one launch per sweep, rows published through per-row
+flags) and the level form (one launch per level) stream the same rows with
+the same threads per row and sum in the same order, so their results must be
+bitwise identical, and the timed choice between them (the first four
+applications alternate) must not change any result.  The bounded waits of
+the sync-free form are checked by a sweep whose dependency is never
+published: the wait runs out, the solve reports CPG_ERR_TIMEOUT, and the
+context stays usable."""
+import numpy as np
+import pytest
+import torch
+
+import cpolyg_b200 as cp
+import oracle
+from cases import mesh, rel, to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def bsr(n, bl, seed):
+    m, _, _ = mesh(n, True, 1.0, 2)
+    rp, cl = m.pattern()
+    rng = np.random.default_rng(seed)
+    blocks = rng.standard_normal((len(cl), bl, bl))
+    for i in range(len(rp) - 1):
+        blocks[rp[i]] += np.eye(bl) * (3.0 * bl)
+    return rp, cl, blocks
+
+
+@pytest.mark.parametrize("bl", [6, 10, 24, 40])
+@pytest.mark.parametrize("prec", [cp.F64, cp.F32])
+def test_sweep_forms_are_bitwise_equal(ctx, monkeypatch, bl, prec):
+    rp, cl, blocks = bsr(1500, bl, 40 + bl)
+    A = cp.BlockMatrix.from_host(ctx, rp, cl, blocks, precision=prec)
+    monkeypatch.setenv("CPG_ILU_SWEEP", "syncfree")
+    P1 = cp.BlockILU0(A, precision=prec)
+    monkeypatch.setenv("CPG_ILU_SWEEP", "levels")
+    P2 = cp.BlockILU0(A, precision=prec)
+    monkeypatch.delenv("CPG_ILU_SWEEP")
+    P3 = cp.BlockILU0(A, precision=prec)
+    lib = cp.lib()
+    assert lib.cpg_precond_sweep_form(P1.h) == 1
+    assert lib.cpg_precond_sweep_form(P2.h) == 2
+    assert lib.cpg_precond_sweep_form(P3.h) == 0
+    x = to_dev(np.random.default_rng(bl).standard_normal((len(rp) - 1) * bl))
+    y1 = P1.solve(x.clone())
+    y2 = P2.solve(x.clone())
+    assert torch.equal(y1, y2)
+    for _ in range(6):  # through the timing applications and past the decision
+        assert torch.equal(P3.solve(x.clone()), y1)
+    assert lib.cpg_precond_sweep_form(P3.h) in (1, 2)
+    if prec == cp.F64:
+        assert rel(to_np(y1), oracle.precond_apply(2, rp, cl, blocks, to_np(x))) < 1e-11
+
+
+def test_sync_free_sweep_wait_runs_out_and_reports(ctx):
+    lib = cp.lib()
+    st = lib.cpg_debug_sweep_timeout(ctx.h)
+    assert st == 6, lib.cpg_last_error(ctx.h)  # CPG_ERR_TIMEOUT
+    # the context still works, and the status word was cleared
+    rp, cl, blocks = bsr(300, 6, 3)
+    A = cp.BlockMatrix.from_host(ctx, rp, cl, blocks)
+    P = cp.BlockILU0(A)
+    x = np.random.default_rng(0).standard_normal((len(rp) - 1) * 6)
+    y = to_np(P.solve(to_dev(x)))
+    assert rel(y, oracle.precond_apply(2, rp, cl, blocks, x)) < 1e-11
