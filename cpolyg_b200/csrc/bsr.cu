@@ -63,6 +63,37 @@ struct VecLoad<float, 4> {
     }
 };
 
+// the same vector loads from shared memory (plain loads: the streaming
+// cache hints above are global-memory instructions)
+template <class T, int VEC>
+struct SmemLoad;
+template <>
+struct SmemLoad<double, 2> {
+    static __device__ __forceinline__ void ld(const double *p, double *v) {
+        const double2 a = *reinterpret_cast<const double2 *>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+    }
+};
+template <>
+struct SmemLoad<float, 2> {
+    static __device__ __forceinline__ void ld(const float *p, double *v) {
+        const float2 a = *reinterpret_cast<const float2 *>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+    }
+};
+template <>
+struct SmemLoad<float, 4> {
+    static __device__ __forceinline__ void ld(const float *p, double *v) {
+        const float4 a = *reinterpret_cast<const float4 *>(p);
+        v[0] = a.x;
+        v[1] = a.y;
+        v[2] = a.z;
+        v[3] = a.w;
+    }
+};
+
 constexpr int MAX_ROW_BLOCKS = 64;
 
 template <class T, int BL, int VEC, int TPR>
@@ -165,14 +196,34 @@ __global__ void __launch_bounds__(256) k_rows_dyn(int BL, int G, const int *__re
 
 // ---------------------------------------------------------------------------
 // Sync-free triangular sweep: one launch for a whole forward or backward
-// ILU(0) sweep.  CTAs claim rows in level order from a counter; a row first
-// waits until every row it reads (its L columns, or its U columns) has
-// published its value (flags[j] == gen), then computes exactly as k_rows and
-// publishes its own.  A CTA only ever waits on rows claimed before its own,
-// by CTAs that are running, so the sweep always progresses; every wait is
-// bounded and reports through err instead of hanging.
+// ILU(0) sweep, warp specialised around a TMA bulk-copy ring.
+//
+// One CTA per SM.  A producer thread claims rows in level order from a
+// global counter and, for each row, copies its contiguous value array
+// (chunks of BPC blocks) from HBM into a ring of R shared-memory stages with
+// cp.async.bulk; an mbarrier per stage signals "full" when the bytes have
+// landed, and one per stage collects the consumer warps' "empty" arrivals.
+// The consumer warps take the stages in order: for each block of a chunk one
+// warp waits until the row it reads has published its value (flags[j] ==
+// gen), then stages that row's x segment in shared memory; after a named
+// barrier every consumer thread streams its elements of the chunk exactly
+// as k_rows does (same threads per row, same element sequence, same group
+// reduction), so the result is bitwise that of the level form.  At the
+// row's last chunk the groups are reduced, x_i is written through L2 and the
+// row's flag is released.  The producer runs up to R chunks ahead, so the
+// copies of later rows overlap the waits, reductions and publishes of the
+// current one.
+//
+// Progress: a consumer only waits on rows claimed before its own, by CTAs
+// that are running and take their rows in claim order.  Every wait is
+// bounded; once any wait gives up it sets *err, later dependency waits stop
+// waiting (the result is then garbage, and the solve reports
+// CPG_ERR_TIMEOUT), and the ring keeps draining so the kernel ends.  A
+// consumer or producer whose own mbarrier wait gives up leaves the loop;
+// the producer then waits (bounded) for the copies it still has in flight.
 // ---------------------------------------------------------------------------
-constexpr long long SWEEP_MAX_SPINS = 1LL << 22;  // x >= 64 ns sleeps: >= 0.27 s
+constexpr long long SWEEP_MAX_SPINS = 1LL << 22;  // dependency polls (>= 64 ns apart): >= 0.27 s
+constexpr long long RING_MAX_SPINS = 1LL << 24;   // mbarrier polls, a backstop only
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
     int v;
@@ -182,39 +233,213 @@ __device__ __forceinline__ int ld_acquire(const int *p) {
 __device__ __forceinline__ void st_release(int *p, int v) {
     asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, int count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// bounded wait for the phase of parity `parity` (>= 1 s before it gives up,
+// longer than a dependency wait can last); false if it gave up
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int *err) {
+    long long spins = 0;
+    while (!mbar_test(bar, parity)) {
+        if (++spins > RING_MAX_SPINS) {
+            atomicExch(err, 2);
+            return false;
+        }
+        if (spins > 1024) __nanosleep(64);
+    }
+    return true;
+}
+// HBM -> shared bulk copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ int lane_of(int tid) { return tid & 31; }
+__device__ __forceinline__ void consumers_sync(int nthreads) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+// the same barrier, returning whether any participating thread passed pred != 0
+__device__ __forceinline__ int consumers_sync_or(int nthreads, int pred) {
+    int r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.s32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.s32 %0, 1, 0, q;\n}"
+        : "=r"(r)
+        : "r"(pred), "r"(nthreads)
+        : "memory");
+    return r;
+}
 
-template <class T, int BL, int VEC, int TPR>
-__global__ void __launch_bounds__(TPR) k_sweep(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
-                                               const int *__restrict__ col, const T *__restrict__ vals, double *x,
-                                               int mode, int *flags, int gen, int *counter, int *err) {
-    static_assert((TPR * VEC) % BL == 0, "stride must be a multiple of the block size");
-    static_assert(BL % VEC == 0, "vector width must divide the block size");
-    static_assert(TPR >= 64, "the claiming thread lives in the second warp");
-    constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
-    constexpr int CLAIMER = 32;  // warp 0 holds the dependency waits
-    __shared__ int s_row[2];
-    __shared__ int scol[MAX_ROW_BLOCKS];
-    __shared__ double red[G][BL];
+// Per-(block size, precision) shape of the sweep: consumer threads CT and
+// vector width VEC match the level form's threads per row (k_rows variant
+// 1), and a chunk of BPC blocks is a whole number of passes of CT * VEC
+// elements, so every thread sees the same element sequence as in k_rows.
+template <class T, int BL>
+struct SweepShape;
+template <class T> struct SweepShape<T, 6> { static constexpr int VEC = 2, CT = 192, BPC = 32, R = 16; };
+template <class T> struct SweepShape<T, 10> { static constexpr int VEC = 2, CT = 320, BPC = 32, R = sizeof(T) == 8 ? 7 : 14; };
+template <> struct SweepShape<double, 24> { static constexpr int VEC = 2, CT = 384, BPC = 4, R = 9; };
+template <> struct SweepShape<float, 24> { static constexpr int VEC = 4, CT = 192, BPC = 8, R = 9; };
+template <> struct SweepShape<double, 40> { static constexpr int VEC = 2, CT = 320, BPC = 2, R = 7; };
+template <> struct SweepShape<float, 40> { static constexpr int VEC = 4, CT = 320, BPC = 4, R = 7; };
+
+template <int BPC>
+struct ChunkMeta {
+    int row;   // cell row, or -1: no more rows
+    int blk0;  // index of the chunk's first block within the row
+    int nb;    // blocks in the chunk
+    int last;  // 1 on the row's last chunk
+    int cols[BPC];
+};
+
+template <class T, int BL>
+struct SweepSmem {
+    using Sh = SweepShape<T, BL>;
+    static constexpr int BL2 = BL * BL, G = Sh::CT * Sh::VEC / BL;
+    static constexpr size_t STAGE = (size_t)Sh::BPC * BL2 * sizeof(T);
+    static constexpr size_t RING = STAGE * Sh::R;
+    static constexpr size_t BARS = RING;                                           // full[R], empty[R]
+    static constexpr size_t META = BARS + 16 * (size_t)Sh::R;
+    static constexpr size_t RED = (META + sizeof(ChunkMeta<Sh::BPC>) * Sh::R + 15) / 16 * 16;
+    static constexpr size_t XS = RED + sizeof(double) * G * BL;                   // x segments, 2 buffers
+    static constexpr size_t BYTES = XS + sizeof(double) * 2 * Sh::BPC * BL;
+    static_assert(STAGE % 16 == 0, "bulk copies move multiples of 16 bytes");
+    static_assert((Sh::CT * Sh::VEC) % BL == 0, "stride must be a multiple of the block size");
+    static_assert(((size_t)Sh::BPC * BL2) % (Sh::CT * Sh::VEC) == 0, "a chunk is a whole number of passes");
+    static_assert(BYTES <= 227 * 1024, "shared memory per CTA");
+};
+
+template <class T, int BL>
+__global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
+    k_sweep(const int *__restrict__ order, int n, const int *__restrict__ rowptr, const int *__restrict__ col,
+            const T *__restrict__ vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
+    using Sh = SweepShape<T, BL>;
+    using L = SweepSmem<T, BL>;
+    constexpr int CT = Sh::CT, VEC = Sh::VEC, BPC = Sh::BPC, R = Sh::R;
+    constexpr int S = CT * VEC, G = S / BL, BL2 = BL * BL, NCW = CT / 32;
+    extern __shared__ __align__(128) unsigned char sm[];
+    T *ring = (T *)sm;
+    uint64_t *full = (uint64_t *)(sm + L::BARS), *empty = full + R;
+    ChunkMeta<BPC> *meta = (ChunkMeta<BPC> *)(sm + L::META);
+    double(*red)[BL] = (double(*)[BL])(sm + L::RED);
+    double(*xs)[BPC][BL] = (double(*)[BPC][BL])(sm + L::XS);
     const int tid = threadIdx.x;
+    if (tid == 0) {
+        for (int r = 0; r < R; r++) {
+            mbar_init(full + r, 1);
+            mbar_init(empty + r, NCW);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (tid >= CT) {  // ---------------- producer warp ----------------
+        // Rows are claimed CLAIM at a time; lane k < CLAIM fetches row k's
+        // metadata, lanes b < nb the chunk's block columns, lane 0 issues the
+        // mbarrier operations and the copies.  The next claim's atomic is in
+        // flight while the current batch is issued.
+        constexpr int CLAIM = 8;
+        const unsigned FULL = 0xffffffffu;
+        int stage = 0;
+        uint32_t phase = 0;
+        int pending[R];  // lane 0: parity of the fill in flight per stage, -1 none
+#pragma unroll
+        for (int r = 0; r < R; r++) pending[r] = -1;
+        bool ok = true, done = false;
+        int qn = (lane_of(tid) == 0) ? atomicAdd(counter, CLAIM) : 0;
+        const int lane = lane_of(tid);
+        while (!done && ok) {
+            const int q0 = __shfl_sync(FULL, qn, 0);
+            if (lane == 0 && q0 < n) qn = atomicAdd(counter, CLAIM);
+            int my_i = -1, my_k0 = 0, my_nb = 0;
+            if (lane < CLAIM && q0 + lane < n) {
+                my_i = order[q0 + lane];
+                my_k0 = rowptr[my_i];
+                my_nb = rowptr[my_i + 1] - my_k0;
+            }
+            for (int k = 0; k < CLAIM && ok && !done; k++) {
+                const int i = __shfl_sync(FULL, my_i, k);
+                const int k0 = __shfl_sync(FULL, my_k0, k), nblk = __shfl_sync(FULL, my_nb, k);
+                done = i < 0;  // past the last row: this chunk is the stop marker
+                int c0 = 0;
+                do {  // a row without blocks still sends one (empty) chunk to publish its flag
+                    const int w = lane == 0 ? (int)mbar_wait(empty + stage, phase ^ 1, err) : 0;
+                    if (!(ok = __shfl_sync(FULL, w, 0) != 0)) break;
+                    ChunkMeta<BPC> &m = meta[stage];
+                    const int nb = done ? 0 : min(BPC, nblk - c0);
+                    for (int b = lane; b < nb; b += 32) m.cols[b] = col[k0 + c0 + b];
+                    __syncwarp();
+                    if (lane == 0) {
+                        m.row = i;
+                        m.blk0 = c0;
+                        m.nb = nb;
+                        m.last = (c0 + nb >= nblk) ? 1 : 0;
+                        if (nb > 0) {
+                            const uint32_t bytes = (uint32_t)(nb * BL2 * sizeof(T));
+                            mbar_arrive_tx(full + stage, bytes);
+                            bulk_load(ring + (size_t)stage * BPC * BL2, vals + (size_t)(k0 + c0) * BL2, bytes,
+                                      full + stage);
+                        } else {
+                            mbar_arrive(full + stage);
+                        }
+                        pending[stage] = (int)phase;
+                    }
+                    __syncwarp();
+                    c0 += BPC;
+                    if (++stage == R) {
+                        stage = 0;
+                        phase ^= 1;
+                    }
+                } while (c0 < nblk);
+            }
+        }
+        if (!ok && lane == 0)  // consumers left early: let the copies in flight land before the CTA ends
+            for (int r = 0; r < R; r++)
+                if (pending[r] >= 0) mbar_wait(full + r, (uint32_t)pending[r], err);
+        return;
+    }
+
+    // ---------------- consumer warps ----------------
+    const int warp = tid >> 5, lane = tid & 31;
     const int e0 = tid * VEC;
     const int r0 = e0 % BL, g = e0 / BL;
     const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
     const double sr = -1.0;
-    if (tid == CLAIMER) s_row[0] = atomicAdd(counter, 1);
-    __syncthreads();
-    for (int cur = 0;; cur ^= 1) {
-        const int q = s_row[cur];
-        if (q >= n) break;
-        // claim the next row now, so the atomic's round trip hides behind this row
-        if (tid == CLAIMER) s_row[cur ^ 1] = atomicAdd(counter, 1);
-        const int i = order[q];
-        const int k0 = rowptr[i], nblk = rowptr[i + 1] - k0;
-        // the backward row's first block is D^{-1}_i (its own column)
-        const int first_dep = (mode == MODE_BACKWARD) ? 1 : 0;
-        for (int b = tid; b < nblk; b += TPR) {
-            const int j = col[k0 + b];
-            if (b < MAX_ROW_BLOCKS) scol[b] = j;
-            if (b >= first_dep) {
+    const int first_dep = (mode == MODE_BACKWARD) ? 1 : 0;  // the backward row's block 0 is D^{-1}_i
+    double acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; v++) acc[v] = 0.0;
+    int stage = 0, buf = 0;
+    uint32_t phase = 0;
+    for (;;) {
+        // a thread whose wait gave up touches nothing of the stage; the
+        // reduction barrier below then takes every consumer out together
+        const bool landed = mbar_wait(full + stage, phase, err);
+        const ChunkMeta<BPC> &m = meta[stage];
+        const int i = landed ? m.row : -1;
+        const int blk0 = landed ? m.blk0 : 0, nb = landed ? m.nb : 0, last = landed ? m.last : 0;
+        // dependencies and x segments: block b of the chunk is handled by warp b % NCW
+        for (int b = warp; b < nb; b += NCW) {
+            const int j = m.cols[b];
+            if (lane == 0 && blk0 + b >= first_dep) {
                 long long spins = 0;
                 while (ld_acquire(flags + j) != gen) {
                     // once any wait has given up, nobody waits any more
@@ -225,22 +450,21 @@ __global__ void __launch_bounds__(TPR) k_sweep(const int *__restrict__ order, in
                     __nanosleep(64);
                 }
             }
+            __syncwarp();
+            // values published during this sweep: read through L2, not L1
+            for (int c = lane; c < BL; c += 32) xs[buf][b][c] = __ldcg(x + (size_t)j * BL + c);
         }
-        __syncthreads();
-        double acc[VEC];
-#pragma unroll
-        for (int v = 0; v < VEC; v++) acc[v] = 0.0;
-        const T *base = vals + (size_t)k0 * BL2;
-        const int E = nblk * BL2;
+        // stop marker (row -1) or a ring wait that gave up: every consumer leaves here
+        if (consumers_sync_or(CT, i < 0)) break;
+        const T *base = ring + (size_t)stage * BPC * BL2;
+        const int E = nb * BL2;
         int blk = e0 / BL2, within = e0 % BL2;
 #pragma unroll 4
         for (int e = e0; e < E; e += S) {
             const int c = within / BL;
             double a[VEC];
-            VecLoad<T, VEC>::ld(base + e, a);
-            const int cb = blk < MAX_ROW_BLOCKS ? scol[blk] : col[k0 + blk];
-            // values published during this sweep: read through L2, not L1
-            const double xv = __ldcg(x + (size_t)cb * BL + c) * (blk == 0 ? s0 : sr);
+            SmemLoad<T, VEC>::ld(base + e, a);
+            const double xv = xs[buf][blk][c] * (blk0 + blk == 0 ? s0 : sr);
 #pragma unroll
             for (int v = 0; v < VEC; v++) acc[v] += a[v] * xv;
             within += S;
@@ -249,54 +473,68 @@ __global__ void __launch_bounds__(TPR) k_sweep(const int *__restrict__ order, in
                 blk++;
             }
         }
-#pragma unroll
-        for (int v = 0; v < VEC; v++) red[g][r0 + v] = acc[v];
-        __syncthreads();
-        if (tid < BL) {
-            double s = 0.0;
-#pragma unroll
-            for (int qq = 0; qq < G; qq++) s += red[qq][tid];
-            double *xi = x + (size_t)i * BL;
-            if (mode == MODE_FORWARD) s = __ldcg(xi + tid) + s;
-            __stcg(xi + tid, s);
+        __syncwarp();
+        if (lane == 0) mbar_arrive(empty + stage);  // this warp is done with the stage
+        if (++stage == R) {
+            stage = 0;
+            phase ^= 1;
         }
-        __syncthreads();  // the row's stores (and the next claim) are done
-        if (tid == 0) {
-            __threadfence();
-            st_release(flags + i, gen);
+        buf ^= 1;
+        if (last) {
+#pragma unroll
+            for (int v = 0; v < VEC; v++) {
+                red[g][r0 + v] = acc[v];
+                acc[v] = 0.0;
+            }
+            consumers_sync(CT);
+            if (tid < BL) {
+                double s = 0.0;
+#pragma unroll
+                for (int qq = 0; qq < G; qq++) s += red[qq][tid];
+                double *xi = x + (size_t)i * BL;
+                if (mode == MODE_FORWARD) s = __ldcg(xi + tid) + s;
+                __stcg(xi + tid, s);
+            }
+            consumers_sync(CT);
+            if (tid == 0) {
+                __threadfence();
+                st_release(flags + i, gen);
+            }
         }
     }
 }
 
-template <class T, int BL, int VEC, int TPR>
+template <class T, int BL>
 cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
                             const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
-    int per_sm = 0;
-    CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep<T, BL, VEC, TPR>, TPR, 0));
-    const int grid = std::max(1, std::min(nrows, std::max(1, per_sm) * ctx->num_sms));
+    using L = SweepSmem<T, BL>;
+    constexpr int threads = SweepShape<T, BL>::CT + 32;
+    // set once per device and instantiation (repeating it is harmless)
+    static bool attr_set[64] = {};
+    const bool known = ctx->device >= 0 && ctx->device < 64 && attr_set[ctx->device];
+    if (!known) {
+        CPG_CUDA(ctx, cudaFuncSetAttribute(k_sweep<T, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)L::BYTES));
+        if (ctx->device >= 0 && ctx->device < 64) attr_set[ctx->device] = true;
+    }
+    const int grid = std::max(1, std::min(nrows, ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-    k_sweep<T, BL, VEC, TPR><<<grid, TPR, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
-                                                           counter, err);
+    k_sweep<T, BL><<<grid, threads, L::BYTES, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
+                                                            counter, err);
     return launched(ctx, "sync-free sweep kernel");
 }
 
-// wide rows: a row's latency sits on the sweep's critical path, so each row
-// is streamed by many threads (every thread issues ~1-2 vector loads per block)
 template <class T>
 cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, const int *rowptr, const int *col,
                           const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
-    constexpr bool F32 = std::is_same<T, float>::value;
-#define CPG_SWEEP(BLV, V, TT) \
-    return launch_sweep_cfg<T, BLV, V, TT>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, counter, err)
+    if (nrows <= 0) return CPG_OK;
+#define CPG_SWEEP(BLV) \
+    return launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, counter, err)
     switch (bl) {
-        case 6: CPG_SWEEP(6, 2, 384);
-        case 10: CPG_SWEEP(10, 2, 640);
-        case 24:
-            if constexpr (F32) { CPG_SWEEP(24, 4, 288); }
-            else { CPG_SWEEP(24, 2, 576); }
-        case 40:
-            if constexpr (F32) { CPG_SWEEP(40, 4, 640); }
-            else { CPG_SWEEP(40, 2, 640); }
+        case 6: CPG_SWEEP(6);
+        case 10: CPG_SWEEP(10);
+        case 24: CPG_SWEEP(24);
+        case 40: CPG_SWEEP(40);
         default: return CPG_ERR_UNSUPPORTED;
     }
 #undef CPG_SWEEP
@@ -409,7 +647,9 @@ int tuned_variant(cpg_ctx *ctx, int precision, int bl, int nrows, const int *row
 
 cpg_status launch_rows(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
                        const int *col, const void *vals, const double *x, double *y, int mode) {
-    int variant = 2;  // level sweeps: widest rows
+    // level sweeps: variant 1, the threads per row of the sync-free sweep's
+    // consumers, so both forms sum in the same order
+    int variant = 1;
     if (mode == MODE_MATVEC && rows == nullptr)
         variant = tuned_variant(ctx, precision, bl, nrows, rowptr, col, vals, x, y);
     return launch_rows_v(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode, variant);
