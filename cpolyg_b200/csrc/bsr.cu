@@ -198,29 +198,30 @@ __global__ void __launch_bounds__(256) k_rows_dyn(int BL, int G, const int *__re
 // Sync-free triangular sweep: one launch for a whole forward or backward
 // ILU(0) sweep, warp specialised around a TMA bulk-copy ring.
 //
-// One CTA per SM.  A producer thread claims rows in level order from a
-// global counter and, for each row, copies its contiguous value array
-// (chunks of BPC blocks) from HBM into a ring of R shared-memory stages with
-// cp.async.bulk; an mbarrier per stage signals "full" when the bytes have
-// landed, and one per stage collects the consumer warps' "empty" arrivals.
-// The consumer warps take the stages in order: for each block of a chunk one
-// warp waits until the row it reads has published its value (flags[j] ==
-// gen), then stages that row's x segment in shared memory; after a named
-// barrier every consumer thread streams its elements of the chunk exactly
-// as k_rows does (same threads per row, same element sequence, same group
-// reduction), so the result is bitwise that of the level form.  At the
-// row's last chunk the groups are reduced, x_i is written through L2 and the
-// row's flag is released.  The producer runs up to R chunks ahead, so the
-// copies of later rows overlap the waits, reductions and publishes of the
-// current one.
+// Several CTAs per SM.  In each, a producer warp claims rows in level order
+// from a global counter (a few at a time) and copies each row's contiguous
+// value array, in chunks of BPC blocks, from HBM into a ring of R shared-
+// memory stages with cp.async.bulk; an mbarrier per stage signals "full"
+// when the bytes have landed and one per stage collects the consumer warps'
+// "empty" arrivals.  The consumer warps take the stages in order.  At a
+// row's first chunk they wait, one warp per block, until every row it reads
+// has published its value (flags[j] == gen), and stage those x segments in
+// shared memory; then every consumer thread streams its elements of each
+// chunk exactly as k_rows does (same threads per row, same element
+// sequence, same group reduction), so the result is bitwise that of the
+// level form.  At the row's last chunk the groups are reduced, x_i is
+// written through L2 and the row's flag is released.  The producer runs up
+// to R chunks ahead, so copies overlap the waits, reductions and publishes.
 //
-// Progress: a consumer only waits on rows claimed before its own, by CTAs
-// that are running and take their rows in claim order.  Every wait is
-// bounded; once any wait gives up it sets *err, later dependency waits stop
-// waiting (the result is then garbage, and the solve reports
-// CPG_ERR_TIMEOUT), and the ring keeps draining so the kernel ends.  A
-// consumer or producer whose own mbarrier wait gives up leaves the loop;
-// the producer then waits (bounded) for the copies it still has in flight.
+// Progress: every CTA takes its rows in claim order and a row only waits on
+// rows claimed before it, by CTAs that are running, so the earliest
+// unfinished row can always proceed.  Every wait is bounded; once any wait
+// gives up it sets *err, later dependency waits stop waiting (the result is
+// then garbage and the solve reports CPG_ERR_TIMEOUT), and the ring keeps
+// draining so the kernel ends.  Consumers leave the loop together, through a
+// barrier that ORs "my ring wait gave up / no more rows" over all of them;
+// a producer whose ring wait gave up waits (bounded) for the copies it still
+// has in flight before it returns.
 // ---------------------------------------------------------------------------
 constexpr long long SWEEP_MAX_SPINS = 1LL << 22;  // dependency polls (>= 64 ns apart): >= 0.27 s
 constexpr long long RING_MAX_SPINS = 1LL << 24;   // mbarrier polls, a backstop only
@@ -290,24 +291,26 @@ __device__ __forceinline__ int consumers_sync_or(int nthreads, int pred) {
 
 // Per-(block size, precision) shape of the sweep: consumer threads CT and
 // vector width VEC match the level form's threads per row (k_rows variant
-// 1), and a chunk of BPC blocks is a whole number of passes of CT * VEC
+// 0), and a chunk of BPC blocks is a whole number of passes of CT * VEC
 // elements, so every thread sees the same element sequence as in k_rows.
+// Shared memory stays near 40-50 KB so four or more CTAs share an SM.
+constexpr int SWEEP_MAXB = SWEEP_MAX_ROW_BLOCKS;  // blocks per row the sync-free form accepts
 template <class T, int BL>
 struct SweepShape;
-template <class T> struct SweepShape<T, 6> { static constexpr int VEC = 2, CT = 192, BPC = 32, R = 16; };
-template <class T> struct SweepShape<T, 10> { static constexpr int VEC = 2, CT = 320, BPC = 32, R = sizeof(T) == 8 ? 7 : 14; };
-template <> struct SweepShape<double, 24> { static constexpr int VEC = 2, CT = 384, BPC = 4, R = 9; };
-template <> struct SweepShape<float, 24> { static constexpr int VEC = 4, CT = 192, BPC = 8, R = 9; };
-template <> struct SweepShape<double, 40> { static constexpr int VEC = 2, CT = 320, BPC = 2, R = 7; };
-template <> struct SweepShape<float, 40> { static constexpr int VEC = 4, CT = 320, BPC = 4, R = 7; };
+template <class T> struct SweepShape<T, 6> { static constexpr int VEC = 2, CT = 96, BPC = 16, R = 6; };
+template <class T> struct SweepShape<T, 10> { static constexpr int VEC = 2, CT = 160, BPC = 16, R = sizeof(T) == 8 ? 3 : 6; };
+template <> struct SweepShape<double, 24> { static constexpr int VEC = 2, CT = 192, BPC = 2, R = 4; };
+template <> struct SweepShape<float, 24> { static constexpr int VEC = 4, CT = 96, BPC = 2, R = 6; };
+template <> struct SweepShape<double, 40> { static constexpr int VEC = 2, CT = 160, BPC = 1, R = 3; };
+template <> struct SweepShape<float, 40> { static constexpr int VEC = 4, CT = 160, BPC = 2, R = 3; };
 
-template <int BPC>
 struct ChunkMeta {
     int row;   // cell row, or -1: no more rows
-    int blk0;  // index of the chunk's first block within the row
+    int blk0;  // index of the chunk's first block within the row (0: first chunk)
     int nb;    // blocks in the chunk
     int last;  // 1 on the row's last chunk
-    int cols[BPC];
+    int nblk;  // blocks in the row
+    int cols[SWEEP_MAXB];  // the row's block columns (first chunk only)
 };
 
 template <class T, int BL>
@@ -316,19 +319,19 @@ struct SweepSmem {
     static constexpr int BL2 = BL * BL, G = Sh::CT * Sh::VEC / BL;
     static constexpr size_t STAGE = (size_t)Sh::BPC * BL2 * sizeof(T);
     static constexpr size_t RING = STAGE * Sh::R;
-    static constexpr size_t BARS = RING;                                           // full[R], empty[R]
+    static constexpr size_t BARS = RING;  // full[R], empty[R]
     static constexpr size_t META = BARS + 16 * (size_t)Sh::R;
-    static constexpr size_t RED = (META + sizeof(ChunkMeta<Sh::BPC>) * Sh::R + 15) / 16 * 16;
-    static constexpr size_t XS = RED + sizeof(double) * G * BL;                   // x segments, 2 buffers
-    static constexpr size_t BYTES = XS + sizeof(double) * 2 * Sh::BPC * BL;
+    static constexpr size_t XS = (META + sizeof(ChunkMeta) * Sh::R + 15) / 16 * 16;  // the row's x segments
+    static constexpr size_t RED = XS + sizeof(double) * SWEEP_MAXB * BL;
+    static constexpr size_t BYTES = RED + sizeof(double) * G * BL;
     static_assert(STAGE % 16 == 0, "bulk copies move multiples of 16 bytes");
     static_assert((Sh::CT * Sh::VEC) % BL == 0, "stride must be a multiple of the block size");
     static_assert(((size_t)Sh::BPC * BL2) % (Sh::CT * Sh::VEC) == 0, "a chunk is a whole number of passes");
-    static_assert(BYTES <= 227 * 1024, "shared memory per CTA");
+    static_assert(BYTES <= 60 * 1024, "several CTAs per SM");
 };
 
 template <class T, int BL>
-__global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
+__global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32)
     k_sweep(const int *__restrict__ order, int n, const int *__restrict__ rowptr, const int *__restrict__ col,
             const T *__restrict__ vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
     using Sh = SweepShape<T, BL>;
@@ -338,9 +341,9 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
     extern __shared__ __align__(128) unsigned char sm[];
     T *ring = (T *)sm;
     uint64_t *full = (uint64_t *)(sm + L::BARS), *empty = full + R;
-    ChunkMeta<BPC> *meta = (ChunkMeta<BPC> *)(sm + L::META);
+    ChunkMeta *meta = (ChunkMeta *)(sm + L::META);
+    double(*xs)[BL] = (double(*)[BL])(sm + L::XS);
     double(*red)[BL] = (double(*)[BL])(sm + L::RED);
-    double(*xs)[BPC][BL] = (double(*)[BPC][BL])(sm + L::XS);
     const int tid = threadIdx.x;
     if (tid == 0) {
         for (int r = 0; r < R; r++) {
@@ -353,19 +356,19 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
 
     if (tid >= CT) {  // ---------------- producer warp ----------------
         // Rows are claimed CLAIM at a time; lane k < CLAIM fetches row k's
-        // metadata, lanes b < nb the chunk's block columns, lane 0 issues the
-        // mbarrier operations and the copies.  The next claim's atomic is in
-        // flight while the current batch is issued.
-        constexpr int CLAIM = 8;
+        // metadata, the lanes copy the row's block columns, lane 0 issues
+        // the mbarrier operations and the copies.  The next claim's atomic
+        // is in flight while the current batch is issued.
+        constexpr int CLAIM = 4;
         const unsigned FULL = 0xffffffffu;
+        const int lane = lane_of(tid);
         int stage = 0;
         uint32_t phase = 0;
         int pending[R];  // lane 0: parity of the fill in flight per stage, -1 none
 #pragma unroll
         for (int r = 0; r < R; r++) pending[r] = -1;
         bool ok = true, done = false;
-        int qn = (lane_of(tid) == 0) ? atomicAdd(counter, CLAIM) : 0;
-        const int lane = lane_of(tid);
+        int qn = (lane == 0) ? atomicAdd(counter, CLAIM) : 0;
         while (!done && ok) {
             const int q0 = __shfl_sync(FULL, qn, 0);
             if (lane == 0 && q0 < n) qn = atomicAdd(counter, CLAIM);
@@ -377,20 +380,25 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
             }
             for (int k = 0; k < CLAIM && ok && !done; k++) {
                 const int i = __shfl_sync(FULL, my_i, k);
-                const int k0 = __shfl_sync(FULL, my_k0, k), nblk = __shfl_sync(FULL, my_nb, k);
+                const int k0 = __shfl_sync(FULL, my_k0, k), nblk_raw = __shfl_sync(FULL, my_nb, k);
+                // the host admits no longer rows; a longer one is reported, not read
+                const int nblk = nblk_raw > SWEEP_MAXB ? 0 : nblk_raw;
+                if (lane == 0 && nblk_raw > SWEEP_MAXB) atomicExch(err, 3);
                 done = i < 0;  // past the last row: this chunk is the stop marker
                 int c0 = 0;
                 do {  // a row without blocks still sends one (empty) chunk to publish its flag
                     const int w = lane == 0 ? (int)mbar_wait(empty + stage, phase ^ 1, err) : 0;
                     if (!(ok = __shfl_sync(FULL, w, 0) != 0)) break;
-                    ChunkMeta<BPC> &m = meta[stage];
+                    ChunkMeta &m = meta[stage];
                     const int nb = done ? 0 : min(BPC, nblk - c0);
-                    for (int b = lane; b < nb; b += 32) m.cols[b] = col[k0 + c0 + b];
+                    if (c0 == 0)
+                        for (int b = lane; b < nblk; b += 32) m.cols[b] = col[k0 + b];
                     __syncwarp();
                     if (lane == 0) {
                         m.row = i;
                         m.blk0 = c0;
                         m.nb = nb;
+                        m.nblk = done ? 0 : nblk;
                         m.last = (c0 + nb >= nblk) ? 1 : 0;
                         if (nb > 0) {
                             const uint32_t bytes = (uint32_t)(nb * BL2 * sizeof(T));
@@ -427,35 +435,38 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
     double acc[VEC];
 #pragma unroll
     for (int v = 0; v < VEC; v++) acc[v] = 0.0;
-    int stage = 0, buf = 0;
+    int stage = 0;
     uint32_t phase = 0;
     for (;;) {
-        // a thread whose wait gave up touches nothing of the stage; the
-        // reduction barrier below then takes every consumer out together
+        // a thread whose ring wait gave up touches nothing of the stage; this
+        // barrier takes every consumer out together on that or on the stop marker
         const bool landed = mbar_wait(full + stage, phase, err);
-        const ChunkMeta<BPC> &m = meta[stage];
-        const int i = landed ? m.row : -1;
-        const int blk0 = landed ? m.blk0 : 0, nb = landed ? m.nb : 0, last = landed ? m.last : 0;
-        // dependencies and x segments: block b of the chunk is handled by warp b % NCW
-        for (int b = warp; b < nb; b += NCW) {
-            const int j = m.cols[b];
-            if (lane == 0 && blk0 + b >= first_dep) {
-                long long spins = 0;
-                while (ld_acquire(flags + j) != gen) {
-                    // once any wait has given up, nobody waits any more
-                    if (++spins > SWEEP_MAX_SPINS || ((spins & 255) == 0 && ld_acquire(err) != 0)) {
-                        atomicExch(err, 1);
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-            }
-            __syncwarp();
-            // values published during this sweep: read through L2, not L1
-            for (int c = lane; c < BL; c += 32) xs[buf][b][c] = __ldcg(x + (size_t)j * BL + c);
-        }
-        // stop marker (row -1) or a ring wait that gave up: every consumer leaves here
+        const int i = landed ? meta[stage].row : -1;
         if (consumers_sync_or(CT, i < 0)) break;
+        const ChunkMeta &m = meta[stage];
+        const int blk0 = m.blk0, nb = m.nb, last = m.last;
+        if (blk0 == 0) {
+            // the row's dependencies and x segments, block b by warp b % NCW
+            const int nblk = m.nblk;
+            for (int b = warp; b < nblk; b += NCW) {
+                const int j = m.cols[b];
+                if (lane == 0 && b >= first_dep) {
+                    long long spins = 0;
+                    while (ld_acquire(flags + j) != gen) {
+                        // once any wait has given up, nobody waits any more
+                        if (++spins > SWEEP_MAX_SPINS || ((spins & 255) == 0 && ld_acquire(err) != 0)) {
+                            atomicExch(err, 1);
+                            break;
+                        }
+                        __nanosleep(64);
+                    }
+                }
+                __syncwarp();
+                // values published during this sweep: read through L2, not L1
+                for (int c = lane; c < BL; c += 32) xs[b][c] = __ldcg(x + (size_t)j * BL + c);
+            }
+            consumers_sync(CT);
+        }
         const T *base = ring + (size_t)stage * BPC * BL2;
         const int E = nb * BL2;
         int blk = e0 / BL2, within = e0 % BL2;
@@ -464,7 +475,8 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
             const int c = within / BL;
             double a[VEC];
             SmemLoad<T, VEC>::ld(base + e, a);
-            const double xv = xs[buf][blk][c] * (blk0 + blk == 0 ? s0 : sr);
+            const int gb = blk0 + blk;  // block index within the row
+            const double xv = xs[gb][c] * (gb == 0 ? s0 : sr);
 #pragma unroll
             for (int v = 0; v < VEC; v++) acc[v] += a[v] * xv;
             within += S;
@@ -479,7 +491,6 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
             stage = 0;
             phase ^= 1;
         }
-        buf ^= 1;
         if (last) {
 #pragma unroll
             for (int v = 0; v < VEC; v++) {
@@ -495,7 +506,7 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32, 1)
                 if (mode == MODE_FORWARD) s = __ldcg(xi + tid) + s;
                 __stcg(xi + tid, s);
             }
-            consumers_sync(CT);
+            consumers_sync(CT);  // also: nobody stages the next row's xs before this row is done
             if (tid == 0) {
                 __threadfence();
                 st_release(flags + i, gen);
@@ -511,13 +522,20 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
     constexpr int threads = SweepShape<T, BL>::CT + 32;
     // set once per device and instantiation (repeating it is harmless)
     static bool attr_set[64] = {};
+    static int per_sm[64] = {};
     const bool known = ctx->device >= 0 && ctx->device < 64 && attr_set[ctx->device];
+    int occ = known ? per_sm[ctx->device] : 0;
     if (!known) {
-        CPG_CUDA(ctx, cudaFuncSetAttribute(k_sweep<T, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)L::BYTES));
-        if (ctx->device >= 0 && ctx->device < 64) attr_set[ctx->device] = true;
+        if (L::BYTES > 48 * 1024)
+            CPG_CUDA(ctx, cudaFuncSetAttribute(k_sweep<T, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)L::BYTES));
+        CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep<T, BL>, threads, L::BYTES));
+        if (ctx->device >= 0 && ctx->device < 64) {
+            per_sm[ctx->device] = occ;
+            attr_set[ctx->device] = true;
+        }
     }
-    const int grid = std::max(1, std::min(nrows, ctx->num_sms));
+    const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
     k_sweep<T, BL><<<grid, threads, L::BYTES, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
                                                             counter, err);
@@ -647,9 +665,9 @@ int tuned_variant(cpg_ctx *ctx, int precision, int bl, int nrows, const int *row
 
 cpg_status launch_rows(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
                        const int *col, const void *vals, const double *x, double *y, int mode) {
-    // level sweeps: variant 1, the threads per row of the sync-free sweep's
+    // level sweeps: variant 0, the threads per row of the sync-free sweep's
     // consumers, so both forms sum in the same order
-    int variant = 1;
+    int variant = 0;
     if (mode == MODE_MATVEC && rows == nullptr)
         variant = tuned_variant(ctx, precision, bl, nrows, rowptr, col, vals, x, y);
     return launch_rows_v(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode, variant);

@@ -122,6 +122,7 @@ cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *o
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
                     int *err);
 bool sweep_supported(int bl);
+constexpr int SWEEP_MAX_ROW_BLOCKS = 16;  // longest L or DU row the sync-free sweep takes
 // x = P^{-1} x without the host-side check of the sweep status word, for
 // callers that check once per solve (precond.cu)
 cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x);

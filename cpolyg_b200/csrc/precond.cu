@@ -565,7 +565,10 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     for (int i = 0; i < n; i++) dinv_idx[i] = precision == CPG_F64 ? P->U_rowptr[i] : i;
     const char *sweep_env = std::getenv("CPG_ILU_SWEEP");
     const bool level_sweeps = sweep_env && std::strcmp(sweep_env, "levels") == 0;
-    P->syncfree = ilu && sweep_supported(P->bl) && !level_sweeps;
+    int longest = 0;
+    for (int i = 0; i < n; i++)
+        longest = std::max({longest, P->L_rowptr[i + 1] - P->L_rowptr[i], P->U_rowptr[i + 1] - P->U_rowptr[i]});
+    P->syncfree = ilu && sweep_supported(P->bl) && !level_sweeps && longest <= SWEEP_MAX_ROW_BLOCKS;
     // CPG_ILU_SWEEP=syncfree skips the timing of the two forms
     if (sweep_env && std::strcmp(sweep_env, "syncfree") == 0) P->sweep_mode = 1;
     cpg_status st = CPG_OK;
