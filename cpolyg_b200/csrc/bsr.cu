@@ -680,6 +680,11 @@ cpg_status rows_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *ro
                    const int *col, const void *vals, const double *x, double *y, int mode) {
     return launch_rows(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode);
 }
+cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
+                     const int *col, const void *vals, const double *x, double *y, int mode, int variant) {
+    return launch_rows_v(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode, variant);
+}
+bool rows_tunable(int bl) { return tunable(bl); }
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
                     int *err) {

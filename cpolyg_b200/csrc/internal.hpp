@@ -91,13 +91,13 @@ struct cpg_precond {
     bool syncfree = false;
     int *row_flags_d = nullptr;
     mutable int generation = 0;
-    // sweep form when both are possible (results are bitwise identical):
-    // 0 = still timing (applications alternate between the forms), 1 =
-    // sync-free, 2 = level sweeps
-    mutable int sweep_mode = 0;
-    mutable int tune_count = 0, tune_pending = -1;
-    mutable float tune_ms[2] = {1e30f, 1e30f};
-    mutable cudaEvent_t tune_ev[2] = {nullptr, nullptr};
+    // triangular sweep form: 0 = still timing (applications cycle through
+    // the candidates), 1 = sync-free, 2 = level sweeps with the sync-free
+    // form's threads per row (bitwise the same result as 1), 3 = level
+    // sweeps with the widest rows
+    mutable int sweep_mode = 2;
+    int n_cand = 0, cand[3] = {0, 0, 0};
+    int form_key = -1;  // process-wide key of the decision (block size, precision, size class)
     int64_t nnzL = 0, nnzU = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
 };
@@ -118,6 +118,10 @@ cpg_status mass_solve_scaled(cpg_ctx *ctx, const cpg_equation *eq, const double 
 // launch helpers implemented in bsr.cu / krylov.cu and used across units
 cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y);
 // sync-free triangular sweep over the rows in `order` (bsr.cu)
+// block-row kernel with an explicit threads-per-row variant (bsr.cu)
+cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
+                     const int *col, const void *vals, const double *x, double *y, int mode, int variant);
+bool rows_tunable(int bl);
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
                     int *err);

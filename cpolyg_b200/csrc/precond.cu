@@ -18,6 +18,8 @@
 #include <climits>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 
 #include "internal.hpp"
@@ -349,20 +351,11 @@ cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrow
     return launch_factor<float, double>(ctx, P, A, nrows, rows);
 }
 
-void drop_tune_events(const cpg_precond *P) {
-    for (cudaEvent_t &e : P->tune_ev)
-        if (e) {
-            cudaEventDestroy(e);
-            e = nullptr;
-        }
-}
-
 void free_precond(cpg_precond *P) {
     void *ptrs[] = {P->lrows_d, P->urows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, P->U_rowptr_d, P->U_col_d,
                     P->U_vals, P->dinv64, P->dinv_idx_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d,
                     P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d};
     for (void *p : ptrs) dfree(p);
-    drop_tune_events(P);
 }
 
 }  // namespace
@@ -381,62 +374,111 @@ cpg_status apply_syncfree(cpg_ctx *ctx, const cpg_precond *P, double *x) {
                     MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err);
 }
 
-cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x, int variant) {
     if (P->kind == CPG_PC_ILU0) {
         const int nl = (int)P->lptr.size() - 1;
         for (int l = 0; l < nl; l++) {
             const int cnt = P->lptr[l + 1] - P->lptr[l];
             // rows without lower blocks pass through the forward sweep unchanged
-            CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->lrows_d + P->lptr[l], P->L_rowptr_d, P->L_col_d,
-                            P->L_vals, x, x, MODE_FORWARD));
+            CPG_TRY(rows_op_v(ctx, P->precision, P->bl, cnt, P->lrows_d + P->lptr[l], P->L_rowptr_d, P->L_col_d,
+                              P->L_vals, x, x, MODE_FORWARD, variant));
         }
     }
     const int nu = (int)P->uptr.size() - 1;
     for (int l = 0; l < nu; l++) {
         const int cnt = P->uptr[l + 1] - P->uptr[l];
-        CPG_TRY(rows_op(ctx, P->precision, P->bl, cnt, P->urows_d + P->uptr[l], P->U_rowptr_d, P->U_col_d,
-                        P->U_vals, x, x, MODE_BACKWARD));
+        CPG_TRY(rows_op_v(ctx, P->precision, P->bl, cnt, P->urows_d + P->uptr[l], P->U_rowptr_d, P->U_col_d,
+                          P->U_vals, x, x, MODE_BACKWARD, variant));
     }
     return CPG_OK;
 }
 
-// Picks the faster sweep form on the preconditioner's own rows: the first
-// four applications alternate between the forms (each timed with events on
-// the stream), the fifth reads the timings and settles.  Both forms stream
-// the same rows with the same threads per row and sum in the same order, so
-// the results do not depend on the choice.
+cpg_status apply_form(cpg_ctx *ctx, const cpg_precond *P, double *x, int form) {
+    if (form == 1) return apply_syncfree(ctx, P, x);
+    return apply_levels(ctx, P, x, form == 3 ? 2 : 0);
+}
+
+// process-wide decisions, so every preconditioner of one kind, block size,
+// precision and size class takes the same form (and the same summation order)
+std::mutex g_form_mu;
+std::map<int, int> g_form;
+
+// Picks the fastest sweep form on the preconditioner's own rows before its
+// first application: each candidate runs twice on a scratch copy of the
+// caller's vector, timed with events on the stream, and the fastest is kept
+// for every preconditioner of the same class in the process.  The caller's
+// vector only ever sees the decided form, so a solve's result does not
+// depend on whether it was the one that timed the forms.
 cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
-    if (P->tune_pending >= 0) {
-        float ms = 1e30f;
-        if (cudaEventSynchronize(P->tune_ev[1]) == cudaSuccess &&
-            cudaEventElapsedTime(&ms, P->tune_ev[0], P->tune_ev[1]) == cudaSuccess)
-            P->tune_ms[P->tune_pending] = std::min(P->tune_ms[P->tune_pending], ms);
-        P->tune_pending = -1;
+    const size_t N = (size_t)P->n * P->bl;
+    double *tmp = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    bool timed = cudaMalloc(&tmp, N * sizeof(double)) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
+                 cudaEventCreate(&e1) == cudaSuccess;
+    float best_ms[3] = {1e30f, 1e30f, 1e30f};
+    cpg_status st = CPG_OK;
+    for (int rep = 0; rep < 2 && timed && st == CPG_OK; rep++)
+        for (int c = 0; c < P->n_cand && st == CPG_OK; c++) {
+            float ms = 1e30f;
+            if (cudaMemcpyAsync(tmp, x, N * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess ||
+                cudaEventRecord(e0, ctx->stream) != cudaSuccess) {
+                timed = false;
+                break;
+            }
+            st = apply_form(ctx, P, tmp, P->cand[c]);
+            if (st == CPG_OK && cudaEventRecord(e1, ctx->stream) == cudaSuccess &&
+                cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+                best_ms[c] = std::min(best_ms[c], ms);
+        }
+    (void)cudaGetLastError();
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (tmp) cudaFree(tmp);
+    if (st != CPG_OK) return st;
+    int best = 0;
+    for (int c = 1; c < P->n_cand; c++)
+        if (best_ms[c] < best_ms[best]) best = c;
+    {
+        std::lock_guard<std::mutex> lk(g_form_mu);
+        auto it = g_form.find(P->form_key);
+        if (it == g_form.end()) g_form[P->form_key] = timed ? P->cand[best] : 2;
+        P->sweep_mode = g_form[P->form_key];  // a concurrent first decision wins
     }
-    if (P->tune_count >= 4 || (!P->tune_ev[0] && (cudaEventCreate(&P->tune_ev[0]) != cudaSuccess ||
-                                                  cudaEventCreate(&P->tune_ev[1]) != cudaSuccess))) {
-        (void)cudaGetLastError();
-        P->sweep_mode = P->tune_ms[1] < P->tune_ms[0] ? 2 : 1;
-        drop_tune_events(P);
-        return P->sweep_mode == 1 ? apply_syncfree(ctx, P, x) : apply_levels(ctx, P, x);
+    return apply_form(ctx, P, x, P->sweep_mode);
+}
+
+// the candidates of a new preconditioner, or its form when already decided
+void choose_form(cpg_precond *P, const char *env) {
+    P->sweep_mode = 2;
+    if (P->kind != CPG_PC_ILU0) return;
+    if (env && std::strcmp(env, "levels") == 0) return;
+    if (env && std::strcmp(env, "levels_wide") == 0) {
+        P->sweep_mode = 3;
+        return;
     }
-    const int which = P->tune_count++ % 2;
-    CPG_CUDA(ctx, cudaEventRecord(P->tune_ev[0], ctx->stream));
-    CPG_TRY(which == 0 ? apply_syncfree(ctx, P, x) : apply_levels(ctx, P, x));
-    CPG_CUDA(ctx, cudaEventRecord(P->tune_ev[1], ctx->stream));
-    P->tune_pending = which;
-    return CPG_OK;
+    if (env && std::strcmp(env, "syncfree") == 0 && P->syncfree) {
+        P->sweep_mode = 1;
+        return;
+    }
+    P->n_cand = 0;
+    if (P->syncfree) P->cand[P->n_cand++] = 1;
+    P->cand[P->n_cand++] = 2;
+    if (rows_tunable(P->bl)) P->cand[P->n_cand++] = 3;
+    if (P->n_cand < 2) return;
+    int size_class = 0;
+    while ((1 << size_class) < P->n) size_class++;
+    P->form_key = ((P->bl * 2 + (P->precision == CPG_F32)) << 6) | size_class;
+    std::lock_guard<std::mutex> lk(g_form_mu);
+    auto it = g_form.find(P->form_key);
+    P->sweep_mode = it != g_form.end() ? it->second : 0;
 }
 
 }  // namespace sweep_form
 
 cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
-    if (P->syncfree) {
-        if (P->sweep_mode == 1) return sweep_form::apply_syncfree(ctx, P, x);
-        if (P->sweep_mode == 0) return sweep_form::apply_tuning(ctx, P, x);
-    }
-    return sweep_form::apply_levels(ctx, P, x);
+    if (P->sweep_mode == 0) return sweep_form::apply_tuning(ctx, P, x);
+    return sweep_form::apply_form(ctx, P, x, P->sweep_mode);
 }
 
 cpg_status check_sweep_error(cpg_ctx *ctx, cpg_status st) {
@@ -569,8 +611,7 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     for (int i = 0; i < n; i++)
         longest = std::max({longest, P->L_rowptr[i + 1] - P->L_rowptr[i], P->U_rowptr[i + 1] - P->U_rowptr[i]});
     P->syncfree = ilu && sweep_supported(P->bl) && !level_sweeps && longest <= SWEEP_MAX_ROW_BLOCKS;
-    // CPG_ILU_SWEEP=syncfree skips the timing of the two forms
-    if (sweep_env && std::strcmp(sweep_env, "syncfree") == 0) P->sweep_mode = 1;
+    sweep_form::choose_form(P, sweep_env);
     cpg_status st = CPG_OK;
     if (P->syncfree) {
         st = dmalloc(ctx, &P->row_flags_d, (size_t)n);
@@ -639,7 +680,7 @@ cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
 
 int cpg_precond_sweep_form(const cpg_precond *P) {
     if (!P || P->kind != CPG_PC_ILU0) return 0;
-    return P->syncfree ? P->sweep_mode : 2;
+    return P->sweep_mode;
 }
 
 cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx) {

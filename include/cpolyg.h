@@ -297,11 +297,16 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A);
 cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x_dev);
 void cpg_precond_destroy(cpg_precond *P);
 /* Triangular sweep form of an ILU(0) preconditioner: 1 = sync-free (one
- * launch per sweep), 2 = one launch per level, 0 = not decided yet (the
- * first four applications time both forms; both give bitwise-identical
- * results).  CPG_ILU_SWEEP=levels or =syncfree in the environment when the
- * preconditioner is created forces a form.  No counterpart in the reference
- * (its sweeps are sequential loops, Preconditioners.cpp:125-158).           */
+ * launch per sweep), 2 = one launch per level with the sync-free form's
+ * threads per row (bitwise the same result as 1), 3 = one launch per level
+ * with the widest rows (another summation order), 0 = not decided yet: the
+ * first application times the candidates on a scratch copy of its vector,
+ * then applies the fastest, and the decision holds for every ILU(0)
+ * preconditioner of the process with the same block size, precision and
+ * size class.  CPG_ILU_SWEEP=syncfree, =levels or
+ * =levels_wide in the environment when the preconditioner is created forces
+ * a form.  No counterpart in the reference (its sweeps are sequential
+ * loops, Preconditioners.cpp:125-158).                                      */
 int cpg_precond_sweep_form(const cpg_precond *P);
 /* Failure-detection check of the sync-free sweep: runs a one-row sweep whose
  * dependency is never published, so the row's bounded wait runs out (well
