@@ -184,6 +184,124 @@ __device__ __forceinline__ double *smem_inverse(int BL, double *A, double *B, in
     return src;
 }
 
+// Blocked Gauss-Jordan inverse for block sizes that are multiples of 8,
+// in panels of 8 pivot columns.  Warp 0 eliminates a panel's columns with
+// partial pivoting (largest magnitude, lowest index on ties), updating only
+// the panel's columns, so afterwards the panel holds
+// [A_PP^{-1}; -A_RP A_PP^{-1}] in the swapped row order (P: the panel's
+// pivot rows, R: the others).  The other columns X then take the panel's row
+// swaps and the block Gauss-Jordan update A_X <- [0; A_RX] + panel * A_PX,
+// a rank-8 product on DMMA.  This is the textbook step in block form: the
+// pivots and row swaps are those of the unblocked elimination, only the sums
+// in the X columns are grouped differently.  Column c of the inverse is
+// column perm[c] of A on return; S holds 8 x (BL-8) doubles of scratch.
+template <int BL>
+__device__ __forceinline__ double *smem_inverse_panel(double *A, double *S, int *piv, int *perm, int *s_ok) {
+    static_assert(BL % 8 == 0 && BL - 8 <= FT, "panel inverse shape");
+    constexpr int NW = FT / 32, NX = BL - 8, RT = BL / 8, XT = NX / 8;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    if (tid == 0) *s_ok = 1;
+    for (int K = 0; K < BL; K += 8) {
+        if (warp == 0) {
+            for (int p = K; p < K + 8; p++) {
+                double best = -1.0;
+                int bi = p;
+                for (int r = p + lane; r < BL; r += 32) {
+                    const double a = fabs(A[p * BL + r]);
+                    if (a > best) {
+                        best = a;
+                        bi = r;
+                    }
+                }
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+                    if (ob > best || (ob == best && oi < bi)) {
+                        best = ob;
+                        bi = oi;
+                    }
+                }
+                const int q = bi;
+                if (lane == 0) {
+                    piv[p] = q;
+                    if (!(best > 0.0)) *s_ok = 0;
+                }
+                if (q != p && lane < 8) {  // swap rows p and q inside the panel
+                    double *col = A + (K + lane) * BL;
+                    const double t = col[p];
+                    col[p] = col[q];
+                    col[q] = t;
+                }
+                __syncwarp();
+                const double pv = A[p * BL + p];
+                const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
+                double rp[8];  // pivot row (panel part), scaled
+#pragma unroll
+                for (int c = 0; c < 8; c++) rp[c] = (K + c == p ? 1.0 : A[(K + c) * BL + p]) * inv;
+                __syncwarp();  // the pivot row is read before it is overwritten
+                for (int r = lane; r < BL; r += 32) {
+                    if (r == p) {
+#pragma unroll
+                        for (int c = 0; c < 8; c++) A[(K + c) * BL + p] = rp[c];
+                    } else {
+                        const double f = A[p * BL + r];
+#pragma unroll
+                        for (int c = 0; c < 8; c++) {
+                            double *e = A + (K + c) * BL + r;
+                            *e = (K + c == p ? 0.0 : *e) - f * rp[c];
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        __syncthreads();
+        if (tid < NX) {  // the panel's row swaps on the other columns, one thread per column
+            double *col = A + (tid < K ? tid : tid + 8) * BL;
+            for (int p = K; p < K + 8; p++) {
+                const int q = piv[p];
+                if (q != p) {
+                    const double t = col[p];
+                    col[p] = col[q];
+                    col[q] = t;
+                }
+            }
+        }
+        __syncthreads();
+        for (int o = tid; o < 8 * NX; o += FT) {  // S = A_PX; those rows restart from zero
+            const int x = o >> 3, k = o & 7;
+            double *e = A + (x < K ? x : x + 8) * BL + K + k;
+            S[o] = *e;
+            *e = 0.0;
+        }
+        __syncthreads();
+        {
+            const int g = lane >> 2, t = lane & 3;
+            for (int tile = warp; tile < RT * XT; tile += NW) {
+                const int r0 = (tile % RT) * 8, x0 = (tile / RT) * 8;
+                double *cc = A + (size_t)((x0 < K ? x0 : x0 + 8) + 2 * t) * BL + r0 + g;
+                double d0 = cc[0], d1 = cc[BL];
+                dmma_m8n8k4(d0, d1, A[(K + t) * BL + r0 + g], S[(x0 + g) * 8 + t]);
+                dmma_m8n8k4(d0, d1, A[(K + 4 + t) * BL + r0 + g], S[(x0 + g) * 8 + 4 + t]);
+                cc[0] = d0;
+                cc[BL] = d1;
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        for (int c = 0; c < BL; c++) perm[c] = c;
+        for (int p = BL - 1; p >= 0; p--) {
+            const int q = piv[p], t = perm[p];
+            perm[p] = perm[q];
+            perm[q] = t;
+        }
+    }
+    __syncthreads();
+    return A;
+}
+
 // Product whose output goes straight from the DMMA fragments to global
 // memory (no shared-memory round trip): C = A * B, BL % 8 == 0.
 template <class T>
@@ -300,7 +418,9 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restr
         }
     }
     __syncthreads();
-    const double *Di = smem_inverse(BL, Ah, T, piv, perm, &s_ok);
+    const double *Di;
+    if constexpr (BLC > 0 && BLC % 8 == 0) Di = smem_inverse_panel<(BLC > 0 ? BLC : 8)>(Ah, T, piv, perm, &s_ok);
+    else Di = smem_inverse(BL, Ah, T, piv, perm, &s_ok);
     if (!s_ok && threadIdx.x == 0) {
         atomicExch(flag, 1);
         atomicMin(flag + 1, j);
