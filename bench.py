@@ -49,6 +49,9 @@ def parse():
                     help="Newton tolerance on the residual's L2 norm (reference: 5e-13)")
     ap.add_argument("--reuse-jacobian", type=int, default=0,
                     help="rebuild the Jacobian and preconditioner every k-th Newton iteration (0 = every one)")
+    ap.add_argument("--newton-rtol", type=float, default=None,
+                    help="also stop Newton only once the last update is below this, relative to the stage vector "
+                         "(default: 0 for f64, 1e-10 for mixed, whose FP32-Jacobian Newton converges linearly)")
     ap.add_argument("--requests", type=int, default=512, help="serve: requests in the timed stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate, requests/s")
     ap.add_argument("--slots", type=int, default=8, help="serve: requests in flight at most")
@@ -56,6 +59,8 @@ def parse():
     ap.add_argument("--compare-fp64", type=int, default=0,
                     help="with --precision mixed: steps over which to measure the error against the FP64 path")
     a = ap.parse_args()
+    if a.newton_rtol is None:
+        a.newton_rtol = 1e-10 if a.precision == "mixed" else 0.0
     if a.workload == "irk":
         if a.cells == 100000:
             a.cells = 500000
@@ -82,13 +87,14 @@ def workload(a) -> dict:
                 "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
                 "dt": a.dt, "gmres_m": 40, "gmres_tol": 1e-9, "preconditioner": "stage block Jacobi",
                 "precision": a.precision, "jacobian": "exact", "newton_tol": a.newton_tol,
-                "reuse_jacobian": a.reuse_jacobian,
+                "newton_rtol": a.newton_rtol, "reuse_jacobian": a.reuse_jacobian,
                 "l2": "inputs larger than L2: each stage Jacobian streams ~16 GB per matvec"}
     return {"workload": f"euler-isentropic-vortex periodic [0,10]^2, {a.cells} Voronoi cells (seed 2), p={a.degree}, "
                         f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton {a.newton_tol:g}, {prec}",
             "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
             "dt": a.dt, "gmres_m": 30, "gmres_tol": 1e-10, "preconditioner": "ilu0",
-            "precision": a.precision, "newton_tol": a.newton_tol, "reuse_jacobian": a.reuse_jacobian,
+            "precision": a.precision, "newton_tol": a.newton_tol, "newton_rtol": a.newton_rtol,
+            "reuse_jacobian": a.reuse_jacobian,
             "jacobian": "exact (the reference's A_x entry and own-state neighbour blocks corrected; same residual "
                         "and converged solution, quadratic Newton); the CPU arm runs the reference's Jacobian",
             "l2": "inputs larger than L2: the Jacobian and ILU factors stream ~9 GB each per sweep"}
@@ -249,7 +255,7 @@ def build_problem(a, cp, ctx):
         def make(mixed):
             return cp.IRK(2, eq, pc=cp.PC_STAGE_BJACOBI, precision=cp.F32 if mixed else cp.F64, gmres_m=40,
                           gmres_tol=1e-9, gmres_maxit=20000, flexible=mixed, newton_tol=a.newton_tol,
-                          reuse_jacobian=a.reuse_jacobian)
+                          reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol)
         return eq, make, u0
     seeds = cp.uniform_seeds(2, a.cells, WIDTH, WIDTH)
     mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
@@ -259,7 +265,7 @@ def build_problem(a, cp, ctx):
     def make(mixed):
         return cp.DIRK(3, eq, pc=cp.PC_ILU0, precision=cp.F32 if mixed else cp.F64, gmres_m=30, gmres_tol=1e-10,
                        gmres_maxit=90000, flexible=mixed, newton_tol=a.newton_tol,
-                       reuse_jacobian=a.reuse_jacobian)
+                       reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol)
     return eq, make, u0
 
 

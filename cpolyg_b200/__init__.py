@@ -426,7 +426,8 @@ class TimeStepper:
 
     def __init__(self, eq: Equation, kind: int | None = None, pc: int = PC_ILU0, precision: int = F64,
                  gmres_m: int = 20, gmres_tol: float = 1e-14, gmres_maxit: int = 0, flexible: bool = False,
-                 newton_tol: float = 5e-13, newton_maxit: int = 100, reuse_jacobian: int = 0):
+                 newton_tol: float = 5e-13, newton_maxit: int = 100, reuse_jacobian: int = 0,
+                 newton_rtol: float = 0.0):
         self.eq = eq
         self.ctx = eq.ctx
         self._lib = eq._lib
@@ -441,6 +442,7 @@ class TimeStepper:
         d.newton_tol = newton_tol
         d.newton_maxit = newton_maxit
         d.reuse_jacobian = reuse_jacobian
+        d.newton_rtol = newton_rtol
         h = C.c_void_p()
         self.ctx.check(self._lib.cpg_stepper_create(self.ctx.h, eq.h, C.byref(d), C.byref(h)))
         self.h = h

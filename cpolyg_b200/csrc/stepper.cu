@@ -386,6 +386,7 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
         const double ts = t + dt * S->c[stage];
         int iter;
         int since_build = 0;
+        double upd_rel = INFINITY;  // last Newton update relative to the stage vector
         for (iter = 0; iter < S->d.newton_maxit; iter++) {
             Comb cb{};
             cb.nk = stage + 1;
@@ -400,7 +401,7 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
             double nr;
             CPG_TRY(newton_norm(S, S->r, &nr));
             st->last_newton_residual = nr;
-            if (nr < S->d.newton_tol) break;
+            if (nr < S->d.newton_tol && (S->d.newton_rtol <= 0 || upd_rel < S->d.newton_rtol)) break;
             st->newton_iterations++;
             const bool rebuild = S->d.reuse_jacobian <= 0 || iter == 0 || since_build >= S->d.reuse_jacobian;
             if (rebuild) {
@@ -420,6 +421,12 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
             st->gmres_iterations += ls.iterations;
             st->linear_solves++;
             CPG_TRY(vec_axpby(ctx, N, -1.0, S->dk, 1.0, ks));  // k -= dk
+            if (S->d.newton_rtol > 0) {
+                double nd, nk;
+                CPG_TRY(newton_norm(S, S->dk, &nd));
+                CPG_TRY(newton_norm(S, ks, &nk));
+                upd_rel = nk > 0 ? nd / nk : 0.0;
+            }
         }
         if (iter == S->d.newton_maxit) st->converged = 0;
     }
@@ -447,6 +454,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
     CPG_TRY(vec_fill(ctx, N * s, 0.0, sol));
     st->converged = 1;
     int iter;
+    double upd_rel = INFINITY;  // last Newton update relative to the stage vectors
     for (iter = 0; iter < S->d.newton_maxit; iter++) {
         double rNorm = 0.0;
         if (inv) {
@@ -486,7 +494,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
         }
         rNorm = std::sqrt(rNorm);
         st->last_newton_residual = rNorm;
-        if (rNorm < S->d.newton_tol) break;
+        if (rNorm < S->d.newton_tol && (S->d.newton_rtol <= 0 || upd_rel < S->d.newton_rtol)) break;
         st->newton_iterations++;
         // modified Newton: with reuse_jacobian = r > 0 the stage Jacobians,
         // the coupled matrix and its factorisation are rebuilt every r-th
@@ -545,6 +553,17 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
         st->gmres_iterations += ls.iterations;
         st->linear_solves++;
         CPG_TRY(vec_axpby(ctx, N * s, -1.0, sol, 1.0, K));  // k (or w) -= solution
+        if (S->d.newton_rtol > 0) {
+            double nd2 = 0.0, nk2 = 0.0;
+            for (int i = 0; i < s; i++) {
+                double nd, nk;
+                CPG_TRY(newton_norm(S, sol + i * N, &nd));
+                CPG_TRY(newton_norm(S, K + i * N, &nk));
+                nd2 += nd * nd;
+                nk2 += nk * nk;
+            }
+            upd_rel = nk2 > 0 ? std::sqrt(nd2 / nk2) : 0.0;
+        }
     }
     if (iter == S->d.newton_maxit) st->converged = 0;
     Comb cb{};

@@ -369,6 +369,14 @@ typedef struct {
     int newton_maxit;        /* reference: 100                              */
     int reuse_jacobian;      /* 0 = rebuild J and P every Newton iteration
                                 as the reference; k > 0 = rebuild every k   */
+    double newton_rtol;      /* 0 = the reference's stopping rule alone; r >
+                                0 = also require the last Newton update to
+                                be below r relative to the stage vector (in
+                                the same L2 norm): the reference's residual
+                                norm weights the weak-form residual by the
+                                mass matrix and can pass while an inexact
+                                (FP32-Jacobian) Newton iteration is still
+                                converging                                  */
 } cpg_stepper_desc;
 
 typedef struct {

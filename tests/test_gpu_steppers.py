@@ -21,7 +21,7 @@ def l2rel(a, b):
 
 def run_both(ctx, name, deg, kind, n, width, steps, dt, pc=cp.PC_ILU0, gm=20, gtol=1e-14, gmaxit=90000,
              precision=cp.F64, flexible=False, reuse=0, periodic=True, init=None, codes=None, dirichlet=None,
-             inflow=None, oracle_pc=None, exact=False):
+             inflow=None, oracle_pc=None, exact=False, rtol=0.0):
     # the oracle always runs the reference's Jacobian: an exact-Jacobian GPU
     # run must land on the same converged solution
     ge, oe, _ = equations(ctx, name, deg, n=n, periodic=periodic, width=width, codes=codes, dirichlet=dirichlet,
@@ -31,7 +31,7 @@ def run_both(ctx, name, deg, kind, n, width, steps, dt, pc=cp.PC_ILU0, gm=20, gt
     ostep = oracle.Stepper(oe, kind, pc=pc if oracle_pc is None else oracle_pc, gmres_m=gm, gmres_tol=gtol,
                            gmres_maxit=gmaxit)
     gstep = cp.TimeStepper(ge, kind=kind, pc=pc, precision=precision, gmres_m=gm, gmres_tol=gtol,
-                           gmres_maxit=gmaxit, flexible=flexible, reuse_jacobian=reuse)
+                           gmres_maxit=gmaxit, flexible=flexible, reuse_jacobian=reuse, newton_rtol=rtol)
     uo = u0.copy()
     ug = to_dev(u0).reshape(ge.np, ge.nc, ge.nb)
     t = 0.0
@@ -126,6 +126,17 @@ def test_mixed_precision_dirk3(ctx):
                              precision=cp.F32, flexible=True, init=VORTEX, exact=True)
     assert gs.stats.converged == 1
     assert l2rel(ug, uo) < 1e-8
+
+
+def test_mixed_precision_dirk3_update_rule(ctx):
+    """The FP32-Jacobian Newton iteration converges linearly; requiring the
+    last update to be below 1e-10 of the stage vector (newton_rtol) on top of
+    the reference's residual rule brings the mixed path to the FP64 oracle's
+    converged solution within 1e-10."""
+    ug, uo, gs, _ = run_both(ctx, "euler", 3, cp.STEP_DIRK3, 150, 10.0, 2, 0.05, gm=30, gtol=1e-10,
+                             precision=cp.F32, flexible=True, init=VORTEX, exact=True, rtol=1e-10)
+    assert gs.stats.converged == 1
+    assert l2rel(ug, uo) < 1e-10
 
 
 def test_step_host_matches_device(ctx):
