@@ -116,63 +116,40 @@ __device__ __forceinline__ void store_blk(int BL, const double *src, T *dst) {
 
 constexpr int FT = 320;  // threads per factor CTA: 8 columns x 40 rows of a 40x40 block at a time
 
-// Gauss-Jordan inverse with partial pivoting and one barrier per elimination
-// step.  Every warp finds the pivot of column p by itself (the same reads and
-// the same tie-break, so all warps agree), which removes the barrier a
-// single pivot-searching warp would need.  Each thread owns one row r and
-// the columns cfirst, cfirst + cstep, ...; the row swap is folded into the
-// reads (rows p and q trade places) and the update ping-pongs between two
-// buffers.  Every element sees the same operations in the same order as the
-// textbook in-place version (pivot: largest magnitude, lowest index on ties,
-// as LAPACK's idamax).  The column swaps that undo the pivoting are composed
-// into perm: column c of the inverse is column perm[c] of the returned
-// buffer.  *s_ok is cleared on a zero pivot.
-__device__ __forceinline__ double *smem_inverse(int BL, double *A, double *B, int *piv, int *perm, int *s_ok) {
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int cstep = FT / BL, r = tid % BL, cfirst = tid / BL;
-    const bool owner = cfirst < cstep;
-    if (tid == 0) *s_ok = 1;
-    double *src = A, *dst = B;
-    for (int p = 0; p < BL; p++) {
-        double best = -1.0;
-        int bi = p;
-        for (int rr = p + lane; rr < BL; rr += 32) {
-            const double a = fabs(src[p * BL + rr]);
-            if (a > best) {
-                best = a;
-                bi = rr;
-            }
+// ---------------------------------------------------------------------------
+// Pivot-block inverses, one warp per block (the batched kernel below runs a
+// level's blocks side by side).  Gauss-Jordan with partial pivoting: pivot
+// = largest magnitude, lowest index on ties (LAPACK's idamax rule); the
+// column swaps that undo the pivoting are composed into perm, so column c of
+// the inverse is column perm[c] of the result.  Both return false on a zero
+// pivot.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int warp_argmax_col(const double *A, int BL, int p, double &best_out) {
+    const int lane = threadIdx.x & 31;
+    double best = -1.0;
+    int bi = p;
+    for (int r = p + lane; r < BL; r += 32) {
+        const double a = fabs(A[p * BL + r]);
+        if (a > best) {
+            best = a;
+            bi = r;
         }
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) {
-            const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-            if (ob > best || (ob == best && oi < bi)) {
-                best = ob;
-                bi = oi;
-            }
-        }
-        const int q = bi;
-        if (tid == 0) {
-            piv[p] = q;
-            if (!(best > 0.0)) *s_ok = 0;
-        }
-        const double pv = src[p * BL + q];
-        const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
-        if (owner) {
-            const int rs = (r == q) ? p : r;  // source row after the swap
-            const double f = src[p * BL + rs];
-            for (int c = cfirst; c < BL; c += cstep) {
-                const double rp = (c == p ? 1.0 : src[c * BL + q]) * inv;  // pivot row, scaled
-                dst[c * BL + r] = (r == p) ? rp : (c == p ? 0.0 : src[c * BL + rs]) - f * rp;
-            }
-        }
-        __syncthreads();
-        double *t = src;
-        src = dst;
-        dst = t;
     }
-    if (tid == 0) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+        if (ob > best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+        }
+    }
+    best_out = best;
+    return bi;
+}
+
+__device__ __forceinline__ void warp_compose_perm(int BL, const int *piv, int *perm) {
+    if ((threadIdx.x & 31) == 0) {
         for (int c = 0; c < BL; c++) perm[c] = c;
         for (int p = BL - 1; p >= 0; p--) {
             const int q = piv[p], t = perm[p];
@@ -180,126 +157,122 @@ __device__ __forceinline__ double *smem_inverse(int BL, double *A, double *B, in
             perm[q] = t;
         }
     }
-    __syncthreads();
-    return src;
+    __syncwarp();
 }
 
-// Blocked Gauss-Jordan inverse for block sizes that are multiples of 8,
-// in panels of 8 pivot columns.  Warp 0 eliminates a panel's columns with
-// partial pivoting (largest magnitude, lowest index on ties), updating only
-// the panel's columns, so afterwards the panel holds
-// [A_PP^{-1}; -A_RP A_PP^{-1}] in the swapped row order (P: the panel's
-// pivot rows, R: the others).  The other columns X then take the panel's row
-// swaps and the block Gauss-Jordan update A_X <- [0; A_RX] + panel * A_PX,
-// a rank-8 product on DMMA.  This is the textbook step in block form: the
-// pivots and row swaps are those of the unblocked elimination, only the sums
-// in the X columns are grouped differently.  Column c of the inverse is
-// column perm[c] of A on return; S holds 8 x (BL-8) doubles of scratch.
+// Blocked form for BL % 8 == 0, in panels of 8 pivot columns.  The panel's
+// columns are eliminated first (the unblocked steps restricted to them), so
+// the panel holds [A_PP^{-1}; -A_RP A_PP^{-1}] in the swapped row order (P:
+// the panel's pivot rows, R: the others); the other columns X then take the
+// panel's row swaps and the block update A_X <- [0; A_RX] + panel * A_PX, a
+// rank-8 product on DMMA.  Pivots and swaps are those of the unblocked
+// elimination; only the sums in the X columns are grouped differently.
+// S holds 8 x (BL - 8) doubles of scratch.
 template <int BL>
-__device__ __forceinline__ double *smem_inverse_panel(double *A, double *S, int *piv, int *perm, int *s_ok) {
-    static_assert(BL % 8 == 0 && BL - 8 <= FT, "panel inverse shape");
-    constexpr int NW = FT / 32, NX = BL - 8, RT = BL / 8, XT = NX / 8;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    if (tid == 0) *s_ok = 1;
+__device__ bool warp_inverse_panel(double *A, double *S, int *piv, int *perm) {
+    static_assert(BL % 8 == 0, "panel inverse shape");
+    constexpr int NX = BL - 8, RT = BL / 8, XT = NX / 8;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    bool ok = true;
     for (int K = 0; K < BL; K += 8) {
-        if (warp == 0) {
-            for (int p = K; p < K + 8; p++) {
-                double best = -1.0;
-                int bi = p;
-                for (int r = p + lane; r < BL; r += 32) {
-                    const double a = fabs(A[p * BL + r]);
-                    if (a > best) {
-                        best = a;
-                        bi = r;
-                    }
-                }
-#pragma unroll
-                for (int off = 16; off > 0; off >>= 1) {
-                    const double ob = __shfl_xor_sync(0xffffffffu, best, off);
-                    const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
-                    if (ob > best || (ob == best && oi < bi)) {
-                        best = ob;
-                        bi = oi;
-                    }
-                }
-                const int q = bi;
-                if (lane == 0) {
-                    piv[p] = q;
-                    if (!(best > 0.0)) *s_ok = 0;
-                }
-                if (q != p && lane < 8) {  // swap rows p and q inside the panel
-                    double *col = A + (K + lane) * BL;
-                    const double t = col[p];
-                    col[p] = col[q];
-                    col[q] = t;
-                }
-                __syncwarp();
-                const double pv = A[p * BL + p];
-                const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
-                double rp[8];  // pivot row (panel part), scaled
-#pragma unroll
-                for (int c = 0; c < 8; c++) rp[c] = (K + c == p ? 1.0 : A[(K + c) * BL + p]) * inv;
-                __syncwarp();  // the pivot row is read before it is overwritten
-                for (int r = lane; r < BL; r += 32) {
-                    if (r == p) {
-#pragma unroll
-                        for (int c = 0; c < 8; c++) A[(K + c) * BL + p] = rp[c];
-                    } else {
-                        const double f = A[p * BL + r];
-#pragma unroll
-                        for (int c = 0; c < 8; c++) {
-                            double *e = A + (K + c) * BL + r;
-                            *e = (K + c == p ? 0.0 : *e) - f * rp[c];
-                        }
-                    }
-                }
-                __syncwarp();
+        for (int p = K; p < K + 8; p++) {
+            double best;
+            const int q = warp_argmax_col(A, BL, p, best);
+            ok = ok && best > 0.0;
+            if (lane == 0) piv[p] = q;
+            if (q != p && lane < 8) {  // swap rows p and q inside the panel
+                double *col = A + (K + lane) * BL;
+                const double tt = col[p];
+                col[p] = col[q];
+                col[q] = tt;
             }
+            __syncwarp();
+            const double pv = A[p * BL + p];
+            const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
+            double rp[8];  // pivot row (panel part), scaled
+#pragma unroll
+            for (int c = 0; c < 8; c++) rp[c] = (K + c == p ? 1.0 : A[(K + c) * BL + p]) * inv;
+            __syncwarp();  // the pivot row is read before it is overwritten
+            for (int r = lane; r < BL; r += 32) {
+                if (r == p) {
+#pragma unroll
+                    for (int c = 0; c < 8; c++) A[(K + c) * BL + p] = rp[c];
+                } else {
+                    const double f = A[p * BL + r];
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        double *e = A + (K + c) * BL + r;
+                        *e = (K + c == p ? 0.0 : *e) - f * rp[c];
+                    }
+                }
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        if (tid < NX) {  // the panel's row swaps on the other columns, one thread per column
-            double *col = A + (tid < K ? tid : tid + 8) * BL;
+        for (int x = lane; x < NX; x += 32) {  // the panel's row swaps on the other columns
+            double *col = A + (x < K ? x : x + 8) * BL;
             for (int p = K; p < K + 8; p++) {
                 const int q = piv[p];
                 if (q != p) {
-                    const double t = col[p];
+                    const double tt = col[p];
                     col[p] = col[q];
-                    col[q] = t;
+                    col[q] = tt;
                 }
             }
         }
-        __syncthreads();
-        for (int o = tid; o < 8 * NX; o += FT) {  // S = A_PX; those rows restart from zero
+        __syncwarp();
+        for (int o = lane; o < 8 * NX; o += 32) {  // S = A_PX; those rows restart from zero
             const int x = o >> 3, k = o & 7;
             double *e = A + (x < K ? x : x + 8) * BL + K + k;
             S[o] = *e;
             *e = 0.0;
         }
-        __syncthreads();
-        {
-            const int g = lane >> 2, t = lane & 3;
-            for (int tile = warp; tile < RT * XT; tile += NW) {
-                const int r0 = (tile % RT) * 8, x0 = (tile / RT) * 8;
-                double *cc = A + (size_t)((x0 < K ? x0 : x0 + 8) + 2 * t) * BL + r0 + g;
-                double d0 = cc[0], d1 = cc[BL];
-                dmma_m8n8k4(d0, d1, A[(K + t) * BL + r0 + g], S[(x0 + g) * 8 + t]);
-                dmma_m8n8k4(d0, d1, A[(K + 4 + t) * BL + r0 + g], S[(x0 + g) * 8 + 4 + t]);
-                cc[0] = d0;
-                cc[BL] = d1;
+        __syncwarp();
+        for (int tile = 0; tile < RT * XT; tile++) {
+            const int r0 = (tile % RT) * 8, x0 = (tile / RT) * 8;
+            double *cc = A + (size_t)((x0 < K ? x0 : x0 + 8) + 2 * t) * BL + r0 + g;
+            double d0 = cc[0], d1 = cc[BL];
+            dmma_m8n8k4(d0, d1, A[(K + t) * BL + r0 + g], S[(x0 + g) * 8 + t]);
+            dmma_m8n8k4(d0, d1, A[(K + 4 + t) * BL + r0 + g], S[(x0 + g) * 8 + 4 + t]);
+            cc[0] = d0;
+            cc[BL] = d1;
+        }
+        __syncwarp();
+    }
+    warp_compose_perm(BL, piv, perm);
+    return ok;
+}
+
+// Unblocked form for any block size: the update ping-pongs between A and B
+// with the row swap folded into the reads (rows p and q trade places), so
+// no element is read after it is overwritten.  Returns the result buffer.
+__device__ double *warp_inverse_gj(int BL, double *A, double *B, int *piv, int *perm, bool &ok) {
+    const int lane = threadIdx.x & 31;
+    ok = true;
+    double *src = A, *dst = B;
+    for (int p = 0; p < BL; p++) {
+        double best;
+        const int q = warp_argmax_col(src, BL, p, best);
+        ok = ok && best > 0.0;
+        if (lane == 0) piv[p] = q;
+        const double pv = src[p * BL + q];
+        const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
+        for (int o = lane; o < BL * BL; o += 32) {
+            const int r = o % BL, c = o / BL;
+            const double rp = (c == p ? 1.0 : src[c * BL + q]) * inv;
+            if (r == p) {
+                dst[o] = rp;
+            } else {
+                const int rs = (r == q) ? p : r;
+                dst[o] = (c == p ? 0.0 : src[c * BL + rs]) - src[p * BL + rs] * rp;
             }
         }
-        __syncthreads();
+        __syncwarp();
+        double *tt = src;
+        src = dst;
+        dst = tt;
     }
-    if (tid == 0) {
-        for (int c = 0; c < BL; c++) perm[c] = c;
-        for (int p = BL - 1; p >= 0; p--) {
-            const int q = piv[p], t = perm[p];
-            perm[p] = perm[q];
-            perm[q] = t;
-        }
-    }
-    __syncthreads();
-    return A;
+    warp_compose_perm(BL, piv, perm);
+    return src;
 }
 
 // Product whose output goes straight from the DMMA fragments to global
@@ -341,7 +314,7 @@ __device__ __forceinline__ void stash_blk(int BL2, const double (&v)[PER], doubl
 // One CTA per row j of the level:
 //   for each lower neighbour i < j (ascending):
 //       L_ji = A_ji D_i^{-1}; Ahat_jj -= L_ji A_ij; U_ij = D_i^{-1} A_ij
-//   D_j^{-1} = inv(Ahat_jj)
+// then k_block_inverse forms D_j^{-1} = inv(Ahat_jj) for the whole level.
 // BLC > 0 compiles the block size in: the three blocks of the next lower
 // neighbour are then fetched into registers while the current products run,
 // and with BLC % 8 == 0 the products run on DMMA with U_ij stored straight
@@ -355,12 +328,10 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restr
                                                    TS *Uv, const int *__restrict__ U_rowptr,
                                                    double *dinv, const int *__restrict__ dinv_idx, int *flag) {
     extern __shared__ double sm[];
-    __shared__ int s_ok;
     const int BL = BLC ? BLC : bl_rt;
     const int BL2 = BL * BL;
     const size_t b2 = (size_t)BL2;
     double *Ah = sm, *D = sm + b2, *X = sm + 2 * b2, *Y = sm + 3 * b2, *T = sm + 4 * b2;
-    int *piv = (int *)(sm + 5 * b2), *perm = piv + BL;
     const int j = rows ? rows[blockIdx.x] : blockIdx.x;
     const int p0 = lp_ptr[j], p1 = lp_ptr[j + 1];
     if constexpr (BLC > 0) {
@@ -418,28 +389,64 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restr
         }
     }
     __syncthreads();
+    // Ahat_jj goes to its D^{-1} slot; k_block_inverse inverts it in place
+    double *dj = dinv + (size_t)dinv_idx[j] * b2;
+    for (int o = threadIdx.x; o < BL2; o += FT) dj[o] = Ah[o];
+}
+
+// The level's pivot blocks, one warp each: Ahat_jj (FP64, in its D^{-1}
+// slot) -> D_j^{-1} in place, and into the DU row's first block when the
+// factors are stored in FP32.  WPB warps per CTA, each with its own shared
+// block (plus a second one or the panel scratch).
+template <class TS, int BLC>
+__global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, const int *__restrict__ rows,
+                                                       TS *Uv, const int *__restrict__ U_rowptr, double *dinv,
+                                                       const int *__restrict__ dinv_idx, int *flag) {
+    extern __shared__ double sm[];
+    const int BL = BLC ? BLC : bl_rt;
+    const size_t b2 = (size_t)BL * BL;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wpb = blockDim.x >> 5;
+    const int k = blockIdx.x * wpb + warp;  // this warp's row of the level
+    if (k >= nrows) return;                 // warp-uniform; no block-wide barriers below
+    constexpr bool PANEL = BLC > 0 && BLC % 8 == 0;
+    // doubles per warp: the block, then the panel scratch (8 x (BL-8)) or a
+    // second block, then piv + perm (ints)
+    const size_t second = PANEL ? 8 * (size_t)(BL - 8) : b2;
+    const size_t per_warp = b2 + second + BL;
+    double *A = sm + warp * per_warp, *B = A + b2;
+    int *piv = (int *)(B + second), *perm = piv + BL;
+    const int j = rows ? rows[k] : k;
+    double *dj = dinv + (size_t)dinv_idx[j] * b2;
+    for (int o = lane; o < (int)b2; o += 32) A[o] = dj[o];
+    __syncwarp();
+    bool ok;
     const double *Di;
-    if constexpr (BLC > 0 && BLC % 8 == 0) Di = smem_inverse_panel<(BLC > 0 ? BLC : 8)>(Ah, T, piv, perm, &s_ok);
-    else Di = smem_inverse(BL, Ah, T, piv, perm, &s_ok);
-    if (!s_ok && threadIdx.x == 0) {
+    if constexpr (PANEL) {
+        ok = warp_inverse_panel<(BLC > 0 ? BLC : 8)>(A, B, piv, perm);
+        Di = A;
+    } else {
+        Di = warp_inverse_gj(BL, A, B, piv, perm, ok);
+    }
+    if (!ok && lane == 0) {
         atomicExch(flag, 1);
         atomicMin(flag + 1, j);
     }
-    double *dj = dinv + (size_t)dinv_idx[j] * b2;
     TS *uj = Uv + (size_t)U_rowptr[j] * b2;
     const bool both = (void *)uj != (void *)dj;
-    for (int o = threadIdx.x; o < BL2; o += FT) {
-        const int r = o % BL, c = o / BL;
-        const double v = Di[perm[c] * BL + r];
-        dj[o] = v;
-        if (both) uj[o] = (TS)v;
+    for (int c = 0; c < BL; c++) {
+        const double *src = Di + (size_t)perm[c] * BL;
+        for (int r = lane; r < BL; r += 32) {
+            const double v = src[r];
+            dj[(size_t)c * BL + r] = v;
+            if (both) uj[(size_t)c * BL + r] = (TS)v;
+        }
     }
 }
 
 template <class TA, class TS, int BLC>
 cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
     const int BL = P->bl;
-    const size_t smem = 5 * (size_t)BL * BL * sizeof(double) + 2 * BL * sizeof(int) + 16;
+    const size_t smem = 5 * (size_t)BL * BL * sizeof(double) + 16;
     if ((int)smem > 48 * 1024)  // per launch: contexts on several host threads may share the kernel
         CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS, BLC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
@@ -447,7 +454,20 @@ cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     k_ilu_factor<TA, TS, BLC><<<nrows, FT, smem, ctx->stream>>>(
         BL, rows, (const TA *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
         P->lp_u_d, (TS *)P->L_vals, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
-    return launched(ctx, "ilu factor kernel");
+    CPG_TRY(launched(ctx, "ilu factor kernel"));
+    // pivot-block inverses: up to 4 warps per CTA within 110 KB of shared memory
+    constexpr bool PANEL = BLC > 0 && BLC % 8 == 0;
+    const size_t b2 = (size_t)BL * BL;
+    const size_t per_warp = (b2 + (PANEL ? 8 * (size_t)(BL - 8) : b2) + BL) * sizeof(double);
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
+    const size_t ismem = per_warp * wpb;
+    if (ismem > 227 * 1024) return fail(ctx, CPG_ERR_UNSUPPORTED, "pivot block too large for shared memory");
+    if ((int)ismem > 48 * 1024)
+        CPG_CUDA(ctx, cudaFuncSetAttribute(k_block_inverse<TS, BLC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)ismem));
+    k_block_inverse<TS, BLC><<<(nrows + wpb - 1) / wpb, 32 * wpb, ismem, ctx->stream>>>(
+        BL, nrows, rows, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
+    return launched(ctx, "pivot block inverse kernel");
 }
 
 template <class TA, class TS>
