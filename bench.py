@@ -39,7 +39,9 @@ def parse():
     ap.add_argument("--cells", type=int, default=100000)
     ap.add_argument("--degree", type=int, default=3)
     ap.add_argument("--dt", type=float, default=0.05)
-    ap.add_argument("--precision", default="f64", choices=["f64", "mixed"])
+    ap.add_argument("--precision", default="f64", choices=["f64", "mixed", "pc32"],
+                    help="f64; mixed = FP32 Jacobian and factors with FP64 FGMRES; pc32 = FP64 Jacobian with FP32 "
+                         "factors (FP64 operator, FP32 preconditioner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="dirk3", choices=["dirk3", "irk", "serve"],
@@ -51,7 +53,7 @@ def parse():
                     help="rebuild the Jacobian and preconditioner every k-th Newton iteration (0 = every one)")
     ap.add_argument("--newton-rtol", type=float, default=None,
                     help="also stop Newton only once the last update is below this, relative to the stage vector "
-                         "(default: 0 for f64, 1e-10 for mixed, whose FP32-Jacobian Newton converges linearly)")
+                         "(default: 0, and 1e-9 for mixed, whose FP32-Jacobian Newton converges linearly)")
     ap.add_argument("--requests", type=int, default=512, help="serve: requests in the timed stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate, requests/s")
     ap.add_argument("--slots", type=int, default=8, help="serve: requests in flight at most")
@@ -60,7 +62,7 @@ def parse():
                     help="with --precision mixed: steps over which to measure the error against the FP64 path")
     a = ap.parse_args()
     if a.newton_rtol is None:
-        a.newton_rtol = 1e-10 if a.precision == "mixed" else 0.0
+        a.newton_rtol = 1e-9 if a.precision == "mixed" else 0.0
     if a.workload == "irk":
         if a.cells == 100000:
             a.cells = 500000
@@ -74,7 +76,7 @@ def parse():
 
 
 def workload(a) -> dict:
-    prec = 'FP32 blocks + FGMRES' if a.precision == 'mixed' else 'FP64'
+    prec = {"mixed": "FP32 blocks + FGMRES", "pc32": "FP64 Jacobian + FP32 ILU factors"}.get(a.precision, "FP64")
     if a.workload == "serve":
         return {"workload": f"serving stream: {a.requests} independent solves, Poisson arrivals at {a.rate}/s; 50% "
                             f"advection (p in 1..3, random angle), 50% Euler vortex (p in 2..3, strength 1..5); "
@@ -255,9 +257,10 @@ def build_problem(a, cp, ctx):
         u0 = eq.interp(cp.INIT_DENSITY_BUMP, [0.1, 0.5, 5.0, 5.0, 0.3, GAMMA])
 
         def make(mixed):
-            return cp.IRK(2, eq, pc=cp.PC_STAGE_BJACOBI, precision=cp.F32 if mixed else cp.F64, gmres_m=40,
-                          gmres_tol=1e-9, gmres_maxit=20000, flexible=mixed, newton_tol=a.newton_tol,
-                          reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol)
+            m32 = mixed == "mixed"
+            return cp.IRK(2, eq, pc=cp.PC_STAGE_BJACOBI, precision=cp.F32 if m32 else cp.F64, gmres_m=40,
+                          gmres_tol=1e-9, gmres_maxit=20000, flexible=m32, newton_tol=a.newton_tol,
+                          reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol, pc_f32=mixed == "pc32")
         return eq, make, u0
     seeds = cp.uniform_seeds(2, a.cells, WIDTH, WIDTH)
     mesh = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
@@ -265,9 +268,10 @@ def build_problem(a, cp, ctx):
     u0 = eq.interp(cp.INIT_VORTEX, VORTEX)
 
     def make(mixed):
-        return cp.DIRK(3, eq, pc=cp.PC_ILU0, precision=cp.F32 if mixed else cp.F64, gmres_m=30, gmres_tol=1e-10,
-                       gmres_maxit=90000, flexible=mixed, newton_tol=a.newton_tol,
-                       reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol)
+        m32 = mixed == "mixed"
+        return cp.DIRK(3, eq, pc=cp.PC_ILU0, precision=cp.F32 if m32 else cp.F64, gmres_m=30, gmres_tol=1e-10,
+                       gmres_maxit=90000, flexible=m32, newton_tol=a.newton_tol,
+                       reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol, pc_f32=mixed == "pc32")
     return eq, make, u0
 
 
@@ -356,16 +360,16 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
 
     ctx = cp.Context(local)
-    mixed = a.precision == "mixed"
+    mixed = a.precision == "mixed"  # FP32 Jacobian (matvec in FP32)
     eq, make_stepper, u0 = build_problem(a, cp, ctx)
-    stepper = make_stepper(mixed)
+    stepper = make_stepper(a.precision)
     u = u0.clone()
     stream = torch.cuda.current_stream()
 
     # mixed precision: error against the FP64 GPU path from the same state
     err_fp64 = None
-    if mixed and a.compare_fp64 and rank == 0:
-        ref_stepper = make_stepper(False)
+    if a.precision != "f64" and a.compare_fp64 and rank == 0:
+        ref_stepper = make_stepper("f64")
         ua, ub = u0.clone(), u0.clone()
         tt = 0.0
         for _ in range(a.compare_fp64):
@@ -464,7 +468,9 @@ def run_ours(a):
                               f"its), scaled by cell count")}
         out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
-               "vs_baseline": None, "dtype": "f32 blocks, f64 vectors" if mixed else "f64",
+               "vs_baseline": None,
+               "dtype": {"mixed": "f32 blocks, f64 vectors", "pc32": "f64 blocks, f32 factors, f64 vectors"}.get(
+                   a.precision, "f64"),
                "data": "synthetic (seeded Voronoi mesh, analytic initial data)",
                "config": dict(workload(a), parallelism=f"replicas x{world}"),
                "newton_iterations_per_step": newton / a.steps, "gmres_iterations_per_step": gmres / a.steps,

@@ -427,7 +427,7 @@ class TimeStepper:
     def __init__(self, eq: Equation, kind: int | None = None, pc: int = PC_ILU0, precision: int = F64,
                  gmres_m: int = 20, gmres_tol: float = 1e-14, gmres_maxit: int = 0, flexible: bool = False,
                  newton_tol: float = 5e-13, newton_maxit: int = 100, reuse_jacobian: int = 0,
-                 newton_rtol: float = 0.0):
+                 newton_rtol: float = 0.0, pc_f32: bool = False):
         self.eq = eq
         self.ctx = eq.ctx
         self._lib = eq._lib
@@ -443,6 +443,7 @@ class TimeStepper:
         d.newton_maxit = newton_maxit
         d.reuse_jacobian = reuse_jacobian
         d.newton_rtol = newton_rtol
+        d.pc_f32 = int(pc_f32)
         h = C.c_void_p()
         self.ctx.check(self._lib.cpg_stepper_create(self.ctx.h, eq.h, C.byref(d), C.byref(h)))
         self.h = h

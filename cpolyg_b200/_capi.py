@@ -52,7 +52,7 @@ class StepperDesc(C.Structure):
     _fields_ = [("kind", C.c_int), ("pc_kind", C.c_int), ("matrix_precision", C.c_int), ("gmres_m", C.c_int),
                 ("gmres_tol", C.c_double), ("gmres_maxit", C.c_int), ("flexible", C.c_int),
                 ("newton_tol", C.c_double), ("newton_maxit", C.c_int), ("reuse_jacobian", C.c_int),
-                ("newton_rtol", C.c_double)]
+                ("newton_rtol", C.c_double), ("pc_f32", C.c_int)]
 
 
 class StepStats(C.Structure):

@@ -96,7 +96,7 @@ struct SmemLoad<float, 4> {
 
 constexpr int MAX_ROW_BLOCKS = 64;
 
-template <class T, int BL, int VEC, int TPR, int UB>
+template <class T, int BL, int VEC, int TPR>
 __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, const int *__restrict__ rowptr,
                                               const int *__restrict__ col, const T *__restrict__ vals,
                                               const double *x, double *y, int mode) {
@@ -122,42 +122,20 @@ __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, cons
     int blk = e0 / BL2, within = e0 % BL2;
     const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
     const double sr = (mode == MODE_MATVEC) ? 1.0 : -1.0;
-    // UB passes per batch: all their value loads are issued before any is
-    // used, so a row costs a few HBM round trips (the level sweeps pay that
-    // latency once per level; the matvec runs UB = 1 at higher occupancy).
-    // Accumulation stays in element order for every UB.
-#pragma unroll(UB == 1 ? 4 : 1)
-    for (int e = e0; e < E; e += UB * S) {
-        double a[UB][VEC], xv[UB];
+#pragma unroll 4
+    for (int e = e0; e < E; e += S) {
+        const int c = within / BL;
+        double a[VEC];
+        VecLoad<T, VEC>::ld(base + e, a);
+        const int cb = blk < MAX_ROW_BLOCKS ? scol[blk] : __ldg(col + k0 + blk);
+        const double xv = __ldg(x + (size_t)cb * BL + c) * (blk == 0 ? s0 : sr);
 #pragma unroll
-        for (int u = 0; u < UB; u++) {
-            if (e + u * S < E) {
-                VecLoad<T, VEC>::ld(base + e + u * S, a[u]);
-            } else {
-#pragma unroll
-                for (int v = 0; v < VEC; v++) a[u][v] = 0.0;
-            }
+        for (int v = 0; v < VEC; v++) acc[v] += a[v] * xv;
+        within += S;
+        while (within >= BL2) {
+            within -= BL2;
+            blk++;
         }
-#pragma unroll
-        for (int u = 0; u < UB; u++) {
-            xv[u] = 0.0;
-            if (e + u * S < E) {
-                const int c = within / BL;
-                const int cb = blk < MAX_ROW_BLOCKS ? scol[blk] : __ldg(col + k0 + blk);
-                xv[u] = __ldg(x + (size_t)cb * BL + c) * (blk == 0 ? s0 : sr);
-                within += S;
-                while (within >= BL2) {
-                    within -= BL2;
-                    blk++;
-                }
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < UB; u++)
-            if (e + u * S < E) {
-#pragma unroll
-                for (int v = 0; v < VEC; v++) acc[v] += a[u][v] * xv[u];
-            }
     }
 #pragma unroll
     for (int v = 0; v < VEC; v++) red[g][r0 + v] = acc[v];
@@ -586,29 +564,24 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
     if (nrows <= 0) return CPG_OK;
     cudaStream_t s = ctx->stream;
     constexpr bool F32 = std::is_same<T, float>::value;
-    // triangular sweeps (latency bound, one level at a time) batch their loads
-    const bool batch = mode != MODE_MATVEC;
     // threads per row: variants 0/1/2 use about 8/16/32 column groups; the
     // matvec picks its variant by timing (autotune below), level sweeps take
     // the widest variant because they are latency bound
-#define CPG_ROWS1(BLV, V, TT)                                                                         \
-    if (batch) k_rows<T, BLV, V, TT, (V > 2 ? 4 : 8)><<<nrows, TT, 0, s>>>(rows, rowptr, col, vals, x, y, mode); \
-    else k_rows<T, BLV, V, TT, 1><<<nrows, TT, 0, s>>>(rows, rowptr, col, vals, x, y, mode);
-#define CPG_ROWS3(BLV, V, T0, T1, T2)        \
-    switch (variant) {                       \
-        case 0: CPG_ROWS1(BLV, V, T0) break; \
-        case 1: CPG_ROWS1(BLV, V, T1) break; \
-        default: CPG_ROWS1(BLV, V, T2) break; \
+#define CPG_ROWS3(BLV, V, T0, T1, T2)                                                                    \
+    switch (variant) {                                                                                   \
+        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;  \
+        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;  \
+        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break; \
     }
     switch (bl) {
-        case 1: CPG_ROWS1(1, 1, 32) break;
-        case 3: CPG_ROWS1(3, 1, 96) break;
-        case 4: CPG_ROWS1(4, 2, 64) break;
+        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;
+        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;
+        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;
         case 6: CPG_ROWS3(6, 2, 96, 192, 384) break;
         case 10: CPG_ROWS3(10, 2, 160, 320, 640) break;
         case 12:
-            if constexpr (F32) { CPG_ROWS1(12, 4, 96) }
-            else { CPG_ROWS1(12, 2, 96) }
+            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode);
+            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode);
             break;
         case 24:
             if constexpr (F32) { CPG_ROWS3(24, 4, 96, 192, 288) }
@@ -629,7 +602,6 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
         }
     }
 #undef CPG_ROWS3
-#undef CPG_ROWS1
     return launched(ctx, "block-row kernel");
 }
 

@@ -318,6 +318,9 @@ struct StageOp : LinOp {
     }
 };
 
+// storage precision of the preconditioner's factors
+int pc_precision(const cpg_stepper *S) { return S->d.pc_f32 ? CPG_F32 : S->d.matrix_precision; }
+
 cpg_status newton_norm(cpg_stepper *S, const double *r, double *out) {
     double l2[4];
     CPG_TRY(cpg_l2norm(S->ctx, S->eq, r, l2));
@@ -409,7 +412,7 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
                 if (S->P) {
                     CPG_TRY(cpg_precond_refactor(ctx, S->P, S->J));
                 } else {
-                    CPG_TRY(cpg_precond_create(ctx, S->J, S->d.pc_kind, S->d.matrix_precision, &S->P));
+                    CPG_TRY(cpg_precond_create(ctx, S->J, S->d.pc_kind, pc_precision(S), &S->P));
                 }
                 since_build = 0;
             }
@@ -529,7 +532,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                     S->Acoef_d, dt, S->eq->mass, (double *)S->stage_blocks->vals);
             CPG_TRY(launched(ctx, "stage block kernel"));
             if (S->P) CPG_TRY(cpg_precond_refactor(ctx, S->P, S->stage_blocks));
-            else CPG_TRY(cpg_precond_create(ctx, S->stage_blocks, CPG_PC_BJACOBI, S->d.matrix_precision, &S->P));
+            else CPG_TRY(cpg_precond_create(ctx, S->stage_blocks, CPG_PC_BJACOBI, pc_precision(S), &S->P));
         } else if (!kron && rebuild) {
             CPG_TRY(fill_coupled(S, S->full, S->map_src, S->map_mrow, S->map_s1, S->map_s2, S->map_mc, dt));
             cpg_bsr *pcm = S->full;
@@ -538,7 +541,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                 pcm = S->fullpc;
             }
             if (S->P) CPG_TRY(cpg_precond_refactor(ctx, S->P, pcm));
-            else CPG_TRY(cpg_precond_create(ctx, pcm, S->d.pc_kind, S->d.matrix_precision, &S->P));
+            else CPG_TRY(cpg_precond_create(ctx, pcm, S->d.pc_kind, pc_precision(S), &S->P));
         }
         if (kron) {
             StageOp op;

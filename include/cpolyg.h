@@ -377,6 +377,10 @@ typedef struct {
                                 mass matrix and can pass while an inexact
                                 (FP32-Jacobian) Newton iteration is still
                                 converging                                  */
+    int pc_f32;              /* 1 = store the preconditioner's factors in
+                                FP32 even when the matrix is FP64 (FP64
+                                operator, FP32 preconditioner); 0 = same
+                                precision as the matrix                     */
 } cpg_stepper_desc;
 
 typedef struct {
