@@ -542,12 +542,125 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
     return launched(ctx, "sync-free sweep kernel");
 }
 
+// ---------------------------------------------------------------------------
+// The same sweep without the ring: CTAs of the level form's size (k_rows
+// variant 0) stream their row's values straight from HBM into registers, as
+// k_rows does, and many of them share an SM.  A CTA claims its next row
+// while the current one streams, waits (one thread per block) for the rows
+// it reads, and publishes like k_sweep.  Same threads per row and element
+// order as the level form, so the same bits; same progress argument and the
+// same bounded waits.
+// ---------------------------------------------------------------------------
+template <class T, int BL>
+__global__ void __launch_bounds__(SweepShape<T, BL>::CT)
+    k_sweep_direct(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
+                   const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags,
+                   int gen, int *counter, int *err) {
+    constexpr int TPR = SweepShape<T, BL>::CT, VEC = SweepShape<T, BL>::VEC;
+    constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
+    constexpr int CLAIMER = TPR > 32 ? 32 : 0;  // warp 0 holds the dependency waits
+    __shared__ int s_row[2];
+    __shared__ int scol[SWEEP_MAXB];
+    __shared__ double red[G][BL];
+    const int tid = threadIdx.x;
+    const int e0 = tid * VEC;
+    const int r0 = e0 % BL, g = e0 / BL;
+    const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
+    const double sr = -1.0;
+    const int first_dep = (mode == MODE_BACKWARD) ? 1 : 0;  // the backward row's block 0 is D^{-1}_i
+    if (tid == CLAIMER) s_row[0] = atomicAdd(counter, 1);
+    __syncthreads();
+    for (int cur = 0;; cur ^= 1) {
+        const int q = s_row[cur];
+        if (q >= n) break;
+        if (tid == CLAIMER) s_row[cur ^ 1] = atomicAdd(counter, 1);  // in flight while this row streams
+        const int i = order[q];
+        const int k0 = rowptr[i], nraw = rowptr[i + 1] - k0;
+        const int nblk = nraw > SWEEP_MAXB ? 0 : nraw;  // the host admits no longer rows
+        if (tid == 0 && nraw > SWEEP_MAXB) atomicExch(err, 3);
+        for (int b = tid; b < nblk; b += TPR) {
+            const int j = col[k0 + b];
+            scol[b] = j;
+            if (b >= first_dep) {
+                long long spins = 0;
+                while (ld_acquire(flags + j) != gen) {
+                    if (++spins > SWEEP_MAX_SPINS || ((spins & 255) == 0 && ld_acquire(err) != 0)) {
+                        atomicExch(err, 1);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+        __syncthreads();
+        double acc[VEC];
+#pragma unroll
+        for (int v = 0; v < VEC; v++) acc[v] = 0.0;
+        const T *base = vals + (size_t)k0 * BL2;
+        const int E = nblk * BL2;
+        int blk = e0 / BL2, within = e0 % BL2;
+#pragma unroll 4
+        for (int e = e0; e < E; e += S) {
+            const int c = within / BL;
+            double a[VEC];
+            VecLoad<T, VEC>::ld(base + e, a);
+            // values published during this sweep: read through L2, not L1
+            const double xv = __ldcg(x + (size_t)scol[blk] * BL + c) * (blk == 0 ? s0 : sr);
+#pragma unroll
+            for (int v = 0; v < VEC; v++) acc[v] += a[v] * xv;
+            within += S;
+            while (within >= BL2) {
+                within -= BL2;
+                blk++;
+            }
+        }
+#pragma unroll
+        for (int v = 0; v < VEC; v++) red[g][r0 + v] = acc[v];
+        __syncthreads();
+        if (tid < BL) {
+            double sum = 0.0;
+#pragma unroll
+            for (int qq = 0; qq < G; qq++) sum += red[qq][tid];
+            double *xi = x + (size_t)i * BL;
+            if (mode == MODE_FORWARD) sum = __ldcg(xi + tid) + sum;
+            __stcg(xi + tid, sum);
+        }
+        __syncthreads();  // the row's stores and the next claim are done
+        if (tid == 0) {
+            __threadfence();
+            st_release(flags + i, gen);
+        }
+    }
+}
+
+template <class T, int BL>
+cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
+                                   const T *vals, double *x, int mode, int *flags, int gen, int *counter,
+                                   int *err) {
+    constexpr int threads = SweepShape<T, BL>::CT;
+    static int per_sm[64] = {};
+    const bool cacheable = ctx->device >= 0 && ctx->device < 64;
+    int occ = cacheable ? per_sm[ctx->device] : 0;
+    if (!occ) {
+        CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep_direct<T, BL>, threads, 0));
+        if (cacheable) per_sm[ctx->device] = occ;
+    }
+    const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
+    CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
+    k_sweep_direct<T, BL><<<grid, threads, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
+                                                            counter, err);
+    return launched(ctx, "sync-free sweep kernel (direct)");
+}
+
 template <class T>
 cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, const int *rowptr, const int *col,
-                          const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
+                          const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err,
+                          bool direct) {
     if (nrows <= 0) return CPG_OK;
-#define CPG_SWEEP(BLV) \
-    return launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, counter, err)
+#define CPG_SWEEP(BLV)                                                                                       \
+    return direct ? launch_sweep_direct_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, \
+                                                    counter, err)                                             \
+                  : launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, counter, err)
     switch (bl) {
         case 6: CPG_SWEEP(6);
         case 10: CPG_SWEEP(10);
@@ -687,12 +800,12 @@ cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *
 bool rows_tunable(int bl) { return tunable(bl); }
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
-                    int *err) {
+                    int *err, bool direct) {
     if (precision == CPG_F32)
         return launch_sweep_t<float>(ctx, bl, nrows, order, rowptr, col, (const float *)vals, x, mode, flags, gen,
-                                     counter, err);
+                                     counter, err, direct);
     return launch_sweep_t<double>(ctx, bl, nrows, order, rowptr, col, (const double *)vals, x, mode, flags, gen,
-                                  counter, err);
+                                  counter, err, direct);
 }
 bool sweep_supported(int bl) { return bl == 6 || bl == 10 || bl == 24 || bl == 40; }
 cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y) {

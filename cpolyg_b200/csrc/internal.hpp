@@ -91,12 +91,13 @@ struct cpg_precond {
     bool syncfree = false;
     int *row_flags_d = nullptr;
     mutable int generation = 0;
-    // triangular sweep form: 0 = still timing (applications cycle through
-    // the candidates), 1 = sync-free, 2 = level sweeps with the sync-free
-    // form's threads per row (bitwise the same result as 1), 3 = level
-    // sweeps with the widest rows
+    // triangular sweep form: 0 = not decided (the first application times
+    // the candidates), 1 = sync-free with a TMA ring, 2 = level sweeps with
+    // the sync-free forms' threads per row (bitwise the same result as 1 and
+    // 4), 3 = level sweeps with the widest rows, 4 = sync-free with direct
+    // loads
     mutable int sweep_mode = 2;
-    int n_cand = 0, cand[3] = {0, 0, 0};
+    int n_cand = 0, cand[4] = {0, 0, 0, 0};
     int form_key = -1;  // process-wide key of the decision (block size, precision, size class)
     int64_t nnzL = 0, nnzU = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
@@ -124,7 +125,7 @@ cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *
 bool rows_tunable(int bl);
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
-                    int *err);
+                    int *err, bool direct = false);
 bool sweep_supported(int bl);
 constexpr int SWEEP_MAX_ROW_BLOCKS = 16;  // longest L or DU row the sync-free sweep takes
 // x = P^{-1} x without the host-side check of the sweep status word, for

@@ -299,19 +299,21 @@ void cpg_precond_destroy(cpg_precond *P);
 /* Triangular sweep form of an ILU(0) preconditioner: 1 = sync-free (one
  * launch per sweep), 2 = one launch per level with the sync-free form's
  * threads per row (bitwise the same result as 1), 3 = one launch per level
- * with the widest rows (another summation order), 0 = not decided yet: the
+ * with the widest rows (another summation order), 4 = sync-free with
+ * direct loads (bitwise the same result as 1), 0 = not decided yet: the
  * first application times the candidates on a scratch copy of its vector,
  * then applies the fastest, and the decision holds for every ILU(0)
  * preconditioner of the process with the same block size, precision and
- * size class.  CPG_ILU_SWEEP=syncfree, =levels or
+ * size class.  CPG_ILU_SWEEP=syncfree, =syncfree_direct, =levels or
  * =levels_wide in the environment when the preconditioner is created forces
  * a form.  No counterpart in the reference (its sweeps are sequential
  * loops, Preconditioners.cpp:125-158).                                      */
 int cpg_precond_sweep_form(const cpg_precond *P);
-/* Failure-detection check of the sync-free sweep: runs a one-row sweep whose
- * dependency is never published, so the row's bounded wait runs out (well
- * under ten seconds); returns CPG_ERR_TIMEOUT when the kernel reported it
- * and leaves the context usable.  No counterpart in the reference.          */
+/* Failure-detection check of the sync-free sweeps: runs, for each of the
+ * two sync-free forms, a one-row sweep whose dependency is never published,
+ * so the row's bounded wait runs out (a few seconds each); returns
+ * CPG_ERR_TIMEOUT when both kernels reported it, and leaves the context
+ * usable.  No counterpart in the reference.                                 */
 cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx);
 /* ILU(0) level schedule (row lists by level), for checks:
  *   lower_ptr[levels_lower+1], lower_rows[n], upper_ptr[...], upper_rows[n] */

@@ -40,20 +40,23 @@ def test_sweep_forms_are_bitwise_equal(ctx, monkeypatch, bl, prec):
     P2 = cp.BlockILU0(A, precision=prec)
     monkeypatch.setenv("CPG_ILU_SWEEP", "levels_wide")
     P3 = cp.BlockILU0(A, precision=prec)
+    monkeypatch.setenv("CPG_ILU_SWEEP", "syncfree_direct")
+    P6 = cp.BlockILU0(A, precision=prec)
     monkeypatch.delenv("CPG_ILU_SWEEP")
     P4 = cp.BlockILU0(A, precision=prec)
     lib = cp.lib()
-    assert [lib.cpg_precond_sweep_form(P.h) for P in (P1, P2, P3)] == [1, 2, 3]
+    assert [lib.cpg_precond_sweep_form(P.h) for P in (P1, P2, P3, P6)] == [1, 2, 3, 4]
     x = to_dev(np.random.default_rng(bl).standard_normal((len(rp) - 1) * bl))
     y1 = P1.solve(x.clone())
     y2 = P2.solve(x.clone())
     y3 = P3.solve(x.clone())
-    assert torch.equal(y1, y2)  # same threads per row: same summation order
+    y6 = P6.solve(x.clone())
+    assert torch.equal(y1, y2) and torch.equal(y1, y6)  # same threads per row: same summation order
     assert rel(to_np(y3), to_np(y1)) < (1e-13 if prec == cp.F64 else 1e-6)
     # timed choice (on a scratch copy): the caller only sees the decided form
     y4 = P4.solve(x.clone())
     form = lib.cpg_precond_sweep_form(P4.h)
-    assert form in (1, 2, 3)
+    assert form in (1, 2, 3, 4)
     assert torch.equal(y4, y3 if form == 3 else y1)
     # the decision holds for the next preconditioner of the same class
     P5 = cp.BlockILU0(A, precision=prec)
@@ -62,7 +65,7 @@ def test_sweep_forms_are_bitwise_equal(ctx, monkeypatch, bl, prec):
         assert rel(to_np(y1), oracle.precond_apply(2, rp, cl, blocks, to_np(x))) < 1e-11
 
 
-def test_sync_free_sweep_wait_runs_out_and_reports(ctx):
+def test_sync_free_sweep_waits_run_out_and_report(ctx):
     lib = cp.lib()
     st = lib.cpg_debug_sweep_timeout(ctx.h)
     assert st == 6, lib.cpg_last_error(ctx.h)  # CPG_ERR_TIMEOUT
