@@ -637,6 +637,8 @@ cpg_status cpg_equation_create(cpg_ctx *ctx, const cpg_mesh *mm, const cpg_equat
     (void)nqf;
     eq->n_vqp = (int)vx.size();
     eq->n_faces = (int)f_nbr.size();
+    // Dirichlet faces read the boundary field at time t; nothing else does
+    eq->time_dependent_bc = std::count(f_nbr.begin(), f_nbr.end(), (int)CPG_BC_DIRICHLET) > 0 ? 1 : 0;
     // interpolation pseudo-inverse (MeshFn::interp, MeshFn.cpp:56-145)
     const int mq = p + 1, nq = mq * mq;
     eq->gl_nodes = gauss_nodes(mq);

@@ -46,6 +46,7 @@ struct cpg_equation {
     int *rowptr_d = nullptr, *colidx_d = nullptr;
     int levels_lower = 0, levels_upper = 0;
     int exact_jacobian = 0;
+    int time_dependent_bc = 0;  // some face reads a boundary field at time t
 
     cpg::Geo geo() const {
         return cpg::Geo{n, bb, vq_ptr, vx, vy, vxi, veta, vw, f_ptr, f_nbr, f_blk, f_nx, f_ny,

@@ -5,6 +5,7 @@
 // reference's evaluation order.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -191,6 +192,12 @@ struct cpg_stepper {
     cpg_bsr *stage_blocks = nullptr;        // CPG_PC_STAGE_BJACOBI blocks
     double *Acoef_d = nullptr;
     double *udev = nullptr;                 // device copy for cpg_step_host
+    // explicit steps replayed as a CUDA graph (keyed on the field and dt)
+    cudaGraphExec_t gexec = nullptr;
+    const double *g_u = nullptr;
+    double g_dt = 0.0;
+    uint64_t g_launches = 0;
+    bool g_off = false;
 };
 
 namespace {
@@ -206,6 +213,7 @@ void free_stepper(cpg_stepper *S) {
         v->rowptr_d = v->colidx_d = nullptr;
         delete v;
     }
+    if (S->gexec) cudaGraphExecDestroy(S->gexec);
     void *ptrs[] = {S->work, S->Jstack, S->map_src, S->map_mrow, S->pmap_src, S->pmap_mrow, S->map_s1, S->map_s2,
                     S->map_mc, S->pmap_s1, S->pmap_s2, S->pmap_mc, S->Acoef_d, S->udev};
     for (void *p : ptrs) dfree(p);
@@ -374,6 +382,54 @@ cpg_status explicit_step(cpg_stepper *S, double *u, double dt, double t) {
     CPG_TRY(rk_stage(S, S->cu, t + dt, dt, k4));
     k_rk4_final<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, k1, k2, k3, k4, u);
     return launched(ctx, "rk4 kernel");
+}
+
+// An explicit step is a fixed sequence of kernel launches with no host
+// synchronisation, so it is captured once as a CUDA graph and replayed: one
+// launch per step instead of 13 (RK4), which is what small meshes in a
+// serving mix pay for.  The graph bakes in the field pointer, dt and the
+// stage times, so it is used only when no face reads a time-dependent
+// boundary field, on a context with its own stream, and is re-captured when
+// the field or dt changes.  CPG_GRAPHS=0 turns it off.
+cpg_status explicit_step_graph(cpg_stepper *S, double *u, double dt, double t) {
+    cpg_ctx *ctx = S->ctx;
+    static const bool off_env = [] {
+        const char *e = std::getenv("CPG_GRAPHS");
+        return e && std::strcmp(e, "0") == 0;
+    }();
+    if (S->g_off || off_env || ctx->stream == nullptr || S->eq->time_dependent_bc) return explicit_step(S, u, dt, t);
+    if (!S->gexec || S->g_u != u || S->g_dt != dt) {
+        if (S->gexec) {
+            cudaGraphExecDestroy(S->gexec);
+            S->gexec = nullptr;
+        }
+        const uint64_t before = ctx->launches;
+        cudaGraph_t graph = nullptr;
+        if (cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            (void)cudaGetLastError();
+            S->g_off = true;
+            return explicit_step(S, u, dt, t);
+        }
+        const cpg_status st = explicit_step(S, u, dt, t);
+        const cudaError_t ec = cudaStreamEndCapture(ctx->stream, &graph);
+        const bool ok = st == CPG_OK && ec == cudaSuccess && graph &&
+                        cudaGraphInstantiate(&S->gexec, graph, 0) == cudaSuccess;
+        if (graph) cudaGraphDestroy(graph);
+        const uint64_t captured = ctx->launches - before;  // kernels the graph holds
+        ctx->launches = before;
+        if (!ok) {  // capture refused: run this and later steps directly
+            (void)cudaGetLastError();
+            S->gexec = nullptr;
+            S->g_off = true;
+            return explicit_step(S, u, dt, t);
+        }
+        S->g_launches = captured;
+        S->g_u = u;
+        S->g_dt = dt;
+    }
+    CPG_CUDA(ctx, cudaGraphLaunch(S->gexec, ctx->stream));
+    ctx->launches += S->g_launches;
+    return CPG_OK;
 }
 
 // DIRK::advance (TimeIntegration.cpp:93-151); BackwardEuler is the one-stage
@@ -702,7 +758,7 @@ cpg_status cpg_step(cpg_ctx *ctx, cpg_stepper *S, double *u, double dt, double t
     cpg_step_stats st{};
     st.converged = 1;
     cpg_status rc;
-    if (S->d.kind <= CPG_STEP_RK4) rc = explicit_step(S, u, dt, t);
+    if (S->d.kind <= CPG_STEP_RK4) rc = explicit_step_graph(S, u, dt, t);
     else if (is_irk(S->d.kind)) rc = irk_step(S, u, dt, t, &st);
     else rc = dirk_step(S, u, dt, t, &st);
     if (stats) *stats = st;

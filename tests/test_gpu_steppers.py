@@ -150,3 +150,32 @@ def test_step_host_matches_device(ctx):
         s1.advance(ud, 1e-3, k * 1e-3)
         s2.advance_host(uh, 1e-3, k * 1e-3)
     assert np.array_equal(to_np(ud), uh)
+
+
+def test_explicit_step_graph_replay_matches_direct_launches(ctx):
+    """On a context with its own stream, explicit steps are captured once as a
+    CUDA graph and replayed; the result must equal the directly launched
+    steps of a default-stream context bit for bit, also after dt changes
+    (re-capture)."""
+    import torch
+    ge, oe, _ = equations(ctx, "euler", 2, n=400, periodic=True, width=10.0)
+    u0 = to_dev(oe.interp(*VORTEX)).reshape(ge.np, ge.nc, ge.nb)
+    direct = cp.RK4(ge)
+    ua = u0.clone()
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        sctx = cp.Context(0, stream)
+        gs, _, _ = equations(sctx, "euler", 2, n=400, periodic=True, width=10.0)
+        graphed = cp.RK4(gs)
+        ub = u0.clone()
+        launches0, direct0 = sctx.launches, ctx.launches
+        t = 0.0
+        for dt in (1e-3, 1e-3, 1e-3, 2e-3, 2e-3):
+            direct.advance(ua, dt, t)
+            graphed.advance(ub, dt, t)
+            t += dt
+        stream.synchronize()
+        # the replays count the kernels they hold
+        assert sctx.launches - launches0 == ctx.launches - direct0
+    torch.cuda.synchronize()
+    assert torch.equal(ua, ub)
