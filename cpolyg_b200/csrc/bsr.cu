@@ -551,12 +551,12 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
 // order as the level form, so the same bits; same progress argument and the
 // same bounded waits.
 // ---------------------------------------------------------------------------
-template <class T, int BL>
-__global__ void __launch_bounds__(SweepShape<T, BL>::CT)
+template <class T, int BL, int TPR>
+__global__ void __launch_bounds__(TPR)
     k_sweep_direct(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
                    const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags,
                    int gen, int *counter, int *err) {
-    constexpr int TPR = SweepShape<T, BL>::CT, VEC = SweepShape<T, BL>::VEC;
+    constexpr int VEC = SweepShape<T, BL>::VEC;
     constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
     constexpr int CLAIMER = TPR > 32 ? 32 : 0;  // warp 0 holds the dependency waits
     __shared__ int s_row[2];
@@ -633,34 +633,49 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT)
     }
 }
 
-template <class T, int BL>
+template <class T, int BL, int TPR>
 cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
                                    const T *vals, double *x, int mode, int *flags, int gen, int *counter,
                                    int *err) {
-    constexpr int threads = SweepShape<T, BL>::CT;
     static int per_sm[64] = {};
     const bool cacheable = ctx->device >= 0 && ctx->device < 64;
     int occ = cacheable ? per_sm[ctx->device] : 0;
     if (!occ) {
-        CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep_direct<T, BL>, threads, 0));
+        CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep_direct<T, BL, TPR>, TPR, 0));
         if (cacheable) per_sm[ctx->device] = occ;
     }
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-    k_sweep_direct<T, BL><<<grid, threads, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
-                                                            counter, err);
+    k_sweep_direct<T, BL, TPR><<<grid, TPR, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags,
+                                                             gen, counter, err);
     return launched(ctx, "sync-free sweep kernel (direct)");
 }
 
+// kind 0: TMA ring; kinds 1, 2, 3: direct loads with 1, 2 or 4 times the
+// consumer threads per row (the level form's variants 0, 1, 2)
 template <class T>
 cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, const int *rowptr, const int *col,
                           const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err,
-                          bool direct) {
+                          int kind) {
     if (nrows <= 0) return CPG_OK;
-#define CPG_SWEEP(BLV)                                                                                       \
-    return direct ? launch_sweep_direct_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, \
-                                                    counter, err)                                             \
-                  : launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen, counter, err)
+#define CPG_SWEEP(BLV)                                                                                          \
+    {                                                                                                           \
+        constexpr int CT = SweepShape<T, BLV>::CT;                                                              \
+        switch (kind) {                                                                                         \
+            case 1:                                                                                             \
+                return launch_sweep_direct_cfg<T, BLV, CT>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, \
+                                                           gen, counter, err);                                  \
+            case 2:                                                                                             \
+                return launch_sweep_direct_cfg<T, BLV, 2 * CT>(ctx, nrows, order, rowptr, col, vals, x, mode,    \
+                                                               flags, gen, counter, err);                       \
+            case 3:                                                                                             \
+                return launch_sweep_direct_cfg<T, BLV, 4 * CT>(ctx, nrows, order, rowptr, col, vals, x, mode,    \
+                                                               flags, gen, counter, err);                       \
+            default:                                                                                            \
+                return launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen,       \
+                                                counter, err);                                                  \
+        }                                                                                                       \
+    }
     switch (bl) {
         case 6: CPG_SWEEP(6);
         case 10: CPG_SWEEP(10);
@@ -800,12 +815,12 @@ cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *
 bool rows_tunable(int bl) { return tunable(bl); }
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
-                    int *err, bool direct) {
+                    int *err, int kind) {
     if (precision == CPG_F32)
         return launch_sweep_t<float>(ctx, bl, nrows, order, rowptr, col, (const float *)vals, x, mode, flags, gen,
-                                     counter, err, direct);
+                                     counter, err, kind);
     return launch_sweep_t<double>(ctx, bl, nrows, order, rowptr, col, (const double *)vals, x, mode, flags, gen,
-                                  counter, err, direct);
+                                  counter, err, kind);
 }
 bool sweep_supported(int bl) { return bl == 6 || bl == 10 || bl == 24 || bl == 40; }
 cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y) {

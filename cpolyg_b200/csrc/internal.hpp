@@ -95,10 +95,10 @@ struct cpg_precond {
     // triangular sweep form: 0 = not decided (the first application times
     // the candidates), 1 = sync-free with a TMA ring, 2 = level sweeps with
     // the sync-free forms' threads per row (bitwise the same result as 1 and
-    // 4), 3 = level sweeps with the widest rows, 4 = sync-free with direct
-    // loads
+    // 4), 3 = level sweeps with the widest rows, 4 / 5 / 6 = sync-free with
+    // direct loads and 1 / 2 / 4 times those threads per row (6 sums as 3)
     mutable int sweep_mode = 2;
-    int n_cand = 0, cand[4] = {0, 0, 0, 0};
+    int n_cand = 0, cand[6] = {0, 0, 0, 0, 0, 0};
     int form_key = -1;  // process-wide key of the decision (block size, precision, size class)
     int64_t nnzL = 0, nnzU = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
@@ -126,7 +126,7 @@ cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *
 bool rows_tunable(int bl);
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
-                    int *err, bool direct = false);
+                    int *err, int kind = 0);
 bool sweep_supported(int bl);
 constexpr int SWEEP_MAX_ROW_BLOCKS = 16;  // longest L or DU row the sync-free sweep takes
 // x = P^{-1} x without the host-side check of the sweep status word, for

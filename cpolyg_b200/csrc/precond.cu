@@ -504,14 +504,14 @@ namespace cpg {
 
 namespace sweep_form {
 
-cpg_status apply_syncfree(cpg_ctx *ctx, const cpg_precond *P, double *x, bool direct) {
+cpg_status apply_syncfree(cpg_ctx *ctx, const cpg_precond *P, double *x, int kind) {
     // status word: flag_dev[2] = a wait ran out, flag_dev[4] = row counter
     int *err = ctx->flag_dev + 2, *counter = ctx->flag_dev + 4;
     const int g = ++P->generation;
     CPG_TRY(sweep_op(ctx, P->precision, P->bl, P->n, P->lrows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, x,
-                     MODE_FORWARD, P->row_flags_d, 2 * g - 1, counter, err, direct));
+                     MODE_FORWARD, P->row_flags_d, 2 * g - 1, counter, err, kind));
     return sweep_op(ctx, P->precision, P->bl, P->n, P->urows_d, P->U_rowptr_d, P->U_col_d, P->U_vals, x,
-                    MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err, direct);
+                    MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err, kind);
 }
 
 cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x, int variant) {
@@ -534,7 +534,8 @@ cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x, int varia
 }
 
 cpg_status apply_form(cpg_ctx *ctx, const cpg_precond *P, double *x, int form) {
-    if (form == 1 || form == 4) return apply_syncfree(ctx, P, x, form == 4);
+    if (form == 1) return apply_syncfree(ctx, P, x, 0);
+    if (form >= 4) return apply_syncfree(ctx, P, x, form - 3);
     return apply_levels(ctx, P, x, form == 3 ? 2 : 0);
 }
 
@@ -555,7 +556,7 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool timed = cudaMalloc(&tmp, N * sizeof(double)) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
                  cudaEventCreate(&e1) == cudaSuccess;
-    float best_ms[4] = {1e30f, 1e30f, 1e30f, 1e30f};
+    float best_ms[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     cpg_status st = CPG_OK;
     for (int rep = 0; rep < 2 && timed && st == CPG_OK; rep++)
         for (int c = 0; c < P->n_cand && st == CPG_OK; c++) {
@@ -604,10 +605,20 @@ void choose_form(cpg_precond *P, const char *env) {
         P->sweep_mode = 4;
         return;
     }
+    if (env && std::strncmp(env, "form", 4) == 0) {  // form1 .. form6
+        const int f = std::atoi(env + 4);
+        const bool needs_syncfree = f == 1 || f >= 4;
+        if (f >= 1 && f <= 6 && (!needs_syncfree || P->syncfree)) {
+            P->sweep_mode = f;
+            return;
+        }
+    }
     P->n_cand = 0;
     if (P->syncfree) {
         P->cand[P->n_cand++] = 1;
         P->cand[P->n_cand++] = 4;
+        P->cand[P->n_cand++] = 5;
+        P->cand[P->n_cand++] = 6;
     }
     P->cand[P->n_cand++] = 2;
     if (rows_tunable(P->bl)) P->cand[P->n_cand++] = 3;
@@ -850,7 +861,7 @@ cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx) {
         // both sync-free forms; each must report its own wait running out
         for (int form = 0; form < 2 && st == CPG_OK; form++) {
             st = sweep_op(ctx, CPG_F64, 6, 1, order, rowptr, col, dbuf, dbuf + 36, MODE_FORWARD, flags, 1 + form,
-                          ctx->flag_dev + 4, ctx->flag_dev + 2, form == 1);
+                          ctx->flag_dev + 4, ctx->flag_dev + 2, form);
             st = check_sweep_error(ctx, st);
             if (st == CPG_ERR_TIMEOUT && form == 0) st = CPG_OK;  // go on to the second form
             else if (st == CPG_OK) st = fail(ctx, CPG_ERR_INVALID_ARG, "a sweep wait did not report running out");

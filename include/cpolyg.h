@@ -299,14 +299,15 @@ void cpg_precond_destroy(cpg_precond *P);
 /* Triangular sweep form of an ILU(0) preconditioner: 1 = sync-free (one
  * launch per sweep), 2 = one launch per level with the sync-free form's
  * threads per row (bitwise the same result as 1), 3 = one launch per level
- * with the widest rows (another summation order), 4 = sync-free with
- * direct loads (bitwise the same result as 1), 0 = not decided yet: the
+ * with the widest rows (another summation order), 4 / 5 / 6 = sync-free
+ * with direct loads and 1 / 2 / 4 times form 1's threads per row (4 sums
+ * as 1, 6 as 3), 0 = not decided yet: the
  * first application times the candidates on a scratch copy of its vector,
  * then applies the fastest, and the decision holds for every ILU(0)
  * preconditioner of the process with the same block size, precision and
- * size class.  CPG_ILU_SWEEP=syncfree, =syncfree_direct, =levels or
- * =levels_wide in the environment when the preconditioner is created forces
- * a form.  No counterpart in the reference (its sweeps are sequential
+ * size class.  CPG_ILU_SWEEP=syncfree, =syncfree_direct, =levels,
+ * =levels_wide or =form<N> in the environment when the preconditioner is
+ * created forces a form.  No counterpart in the reference (its sweeps are sequential
  * loops, Preconditioners.cpp:125-158).                                      */
 int cpg_precond_sweep_form(const cpg_precond *P);
 /* Failure-detection check of the sync-free sweeps: runs, for each of the

@@ -42,22 +42,31 @@ def test_sweep_forms_are_bitwise_equal(ctx, monkeypatch, bl, prec):
     P3 = cp.BlockILU0(A, precision=prec)
     monkeypatch.setenv("CPG_ILU_SWEEP", "syncfree_direct")
     P6 = cp.BlockILU0(A, precision=prec)
+    monkeypatch.setenv("CPG_ILU_SWEEP", "form5")
+    P7 = cp.BlockILU0(A, precision=prec)
+    monkeypatch.setenv("CPG_ILU_SWEEP", "form6")
+    P8 = cp.BlockILU0(A, precision=prec)
     monkeypatch.delenv("CPG_ILU_SWEEP")
     P4 = cp.BlockILU0(A, precision=prec)
     lib = cp.lib()
-    assert [lib.cpg_precond_sweep_form(P.h) for P in (P1, P2, P3, P6)] == [1, 2, 3, 4]
+    assert [lib.cpg_precond_sweep_form(P.h) for P in (P1, P2, P3, P6, P7, P8)] == [1, 2, 3, 4, 5, 6]
     x = to_dev(np.random.default_rng(bl).standard_normal((len(rp) - 1) * bl))
     y1 = P1.solve(x.clone())
     y2 = P2.solve(x.clone())
     y3 = P3.solve(x.clone())
     y6 = P6.solve(x.clone())
+    y7 = P7.solve(x.clone())
+    y8 = P8.solve(x.clone())
     assert torch.equal(y1, y2) and torch.equal(y1, y6)  # same threads per row: same summation order
-    assert rel(to_np(y3), to_np(y1)) < (1e-13 if prec == cp.F64 else 1e-6)
+    assert torch.equal(y3, y8)
+    for y in (y3, y7):
+        assert rel(to_np(y), to_np(y1)) < (1e-13 if prec == cp.F64 else 1e-6)
+    expected = {1: y1, 2: y1, 3: y3, 4: y1, 5: y7, 6: y3}
     # timed choice (on a scratch copy): the caller only sees the decided form
     y4 = P4.solve(x.clone())
     form = lib.cpg_precond_sweep_form(P4.h)
-    assert form in (1, 2, 3, 4)
-    assert torch.equal(y4, y3 if form == 3 else y1)
+    assert form in expected
+    assert torch.equal(y4, expected[form])
     # the decision holds for the next preconditioner of the same class
     P5 = cp.BlockILU0(A, precision=prec)
     assert lib.cpg_precond_sweep_form(P5.h) == form
