@@ -301,7 +301,7 @@ void cpg_precond_destroy(cpg_precond *P);
  * threads per row (bitwise the same result as 1), 3 = one launch per level
  * with the widest rows (another summation order), 4 / 5 / 6 = sync-free
  * with direct loads and 1 / 2 / 4 times form 1's threads per row (4 sums
- * as 1, 6 as 3), 0 = not decided yet: the
+ * as 1), 0 = not decided yet: the
  * first application times the candidates on a scratch copy of its vector,
  * then applies the fastest, and the decision holds for every ILU(0)
  * preconditioner of the process with the same block size, precision and
