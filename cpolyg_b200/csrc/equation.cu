@@ -131,7 +131,9 @@ constexpr int VQC = 32;  // volume qp per chunk
 constexpr int FQC = 36;  // face qp per chunk (whole faces)
 
 template <class Phys, int P, class TOut>
-__global__ void __launch_bounds__(JT) k_jacobian(Geo g, Phys ph, BCParams bc, const double *__restrict__ u,
+// at most 168 registers a thread, so three CTAs share an SM (246 unbounded,
+// two CTAs); the few spilled bytes cost less than the lost occupancy
+__global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc, const double *__restrict__ u,
                                                  double t, double scale, int add_mass,
                                                  const double *__restrict__ mass, const int *__restrict__ rowptr,
                                                  TOut *__restrict__ J) {

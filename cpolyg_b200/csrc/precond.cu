@@ -275,24 +275,6 @@ __device__ double *warp_inverse_gj(int BL, double *A, double *B, int *piv, int *
     return src;
 }
 
-// Product whose output goes straight from the DMMA fragments to global
-// memory (no shared-memory round trip): C = A * B, BL % 8 == 0.
-template <class T>
-__device__ __forceinline__ void dmma_gemm_to_global(int BL, const double *A, const double *B, T *C) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    const int nt = BL >> 3;
-    for (int tile = warp; tile < nt * nt; tile += nw) {
-        const int r0 = (tile % nt) * 8, c0 = (tile / nt) * 8;
-        double d0 = 0.0, d1 = 0.0;
-        for (int k = 0; k < BL; k += 4)
-            dmma_m8n8k4(d0, d1, A[(k + t) * BL + r0 + g], B[(c0 + g) * BL + k + t]);
-        T *cc = C + (size_t)(c0 + 2 * t) * BL + r0 + g;
-        cc[0] = (T)d0;
-        cc[BL] = (T)d1;
-    }
-}
-
 // block -> registers (PER elements per thread, element o = tid + k*FT)
 template <int PER, class T>
 __device__ __forceinline__ void fetch_blk(int BL2, const T *src, double (&v)[PER]) {
@@ -311,6 +293,70 @@ __device__ __forceinline__ void stash_blk(int BL2, const double (&v)[PER], doubl
     }
 }
 
+// Padded shared-memory blocks for the DMMA path: column-major with leading
+// dimension LD = BL + 4 doubles.  With LD = BL the fragment loads of the
+// m8n8k4 products hit the same banks 2-way (A operand) and 4-way (B
+// operand); the padding staggers the columns so a half-warp's sixteen
+// 8-byte loads fall in distinct banks.
+template <int BL>
+struct Pad {
+    static constexpr int LD = BL + 4;
+    static __device__ __forceinline__ int at(int o) { return (o / BL) * LD + o % BL; }  // dense index -> padded
+};
+template <int BL, int PER>
+__device__ __forceinline__ void stash_pad(const double (&v)[PER], double *dst) {
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+        const int o = threadIdx.x + k * FT;
+        if (o < BL * BL) dst[Pad<BL>::at(o)] = v[k];
+    }
+}
+template <int BL, class T>
+__device__ __forceinline__ void load_pad(const T *src, double *dst) {
+    for (int o = threadIdx.x; o < BL * BL; o += FT) dst[Pad<BL>::at(o)] = (double)src[o];
+}
+template <int BL, class T>
+__device__ __forceinline__ void store_pad(const double *src, T *dst) {
+    for (int o = threadIdx.x; o < BL * BL; o += FT) dst[o] = (T)src[Pad<BL>::at(o)];
+}
+// C = A * B or C -= A * B on padded blocks (DMMA, 8x8 tiles per warp)
+template <int BL>
+__device__ __forceinline__ void gemm_pad(const double *A, const double *B, double *C, bool sub) {
+    constexpr int LD = Pad<BL>::LD, NT = BL / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = FT / 32;
+    const int g = lane >> 2, t = lane & 3;
+    for (int tile = warp; tile < NT * NT; tile += nw) {
+        const int r0 = (tile % NT) * 8, c0 = (tile / NT) * 8;
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll 5
+        for (int k = 0; k < BL; k += 4) dmma_m8n8k4(d0, d1, A[(k + t) * LD + r0 + g], B[(c0 + g) * LD + k + t]);
+        double *cc = C + (c0 + 2 * t) * LD + r0 + g;
+        if (sub) {
+            cc[0] = cc[0] - d0;
+            cc[LD] = cc[LD] - d1;
+        } else {
+            cc[0] = d0;
+            cc[LD] = d1;
+        }
+    }
+}
+// C (dense, global) = A * B on padded blocks, straight from the fragments
+template <int BL, class T>
+__device__ __forceinline__ void gemm_pad_to_global(const double *A, const double *B, T *C) {
+    constexpr int LD = Pad<BL>::LD, NT = BL / 8;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = FT / 32;
+    const int g = lane >> 2, t = lane & 3;
+    for (int tile = warp; tile < NT * NT; tile += nw) {
+        const int r0 = (tile % NT) * 8, c0 = (tile / NT) * 8;
+        double d0 = 0.0, d1 = 0.0;
+#pragma unroll 5
+        for (int k = 0; k < BL; k += 4) dmma_m8n8k4(d0, d1, A[(k + t) * LD + r0 + g], B[(c0 + g) * LD + k + t]);
+        T *cc = C + (size_t)(c0 + 2 * t) * BL + r0 + g;
+        cc[0] = (T)d0;
+        cc[BL] = (T)d1;
+    }
+}
+
 // One CTA per row j of the level:
 //   for each lower neighbour i < j (ascending):
 //       L_ji = A_ji D_i^{-1}; Ahat_jj -= L_ji A_ij; U_ij = D_i^{-1} A_ij
@@ -320,7 +366,7 @@ __device__ __forceinline__ void stash_blk(int BL2, const double (&v)[PER], doubl
 // and with BLC % 8 == 0 the products run on DMMA with U_ij stored straight
 // from the fragments.  BLC == 0 is the generic path (any block size).
 template <class TA, class TS, int BLC>
-__global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restrict__ rows, const TA *__restrict__ A,
+__global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__restrict__ rows, const TA *__restrict__ A,
                                                    const int *__restrict__ diag_a, const int *__restrict__ lp_ptr,
                                                    const int *__restrict__ lp_i, const int *__restrict__ lp_aji,
                                                    const int *__restrict__ lp_aij, const int *__restrict__ lp_l,
@@ -334,9 +380,40 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restr
     double *Ah = sm, *D = sm + b2, *X = sm + 2 * b2, *Y = sm + 3 * b2, *T = sm + 4 * b2;
     const int j = rows ? rows[blockIdx.x] : blockIdx.x;
     const int p0 = lp_ptr[j], p1 = lp_ptr[j + 1];
-    if constexpr (BLC > 0) {
+    if constexpr (BLC > 0 && BLC % 8 == 0) {  // DMMA on padded blocks
         constexpr int PER = (BLC * BLC + FT - 1) / FT;
-        constexpr bool TC = (BLC % 8) == 0;
+        constexpr int PB = BLC * Pad<BLC>::LD;   // doubles per padded block
+        double *Ap = sm, *Dp = sm + PB, *Xp = sm + 2 * PB, *Yp = sm + 3 * PB, *Tp = sm + 4 * PB;
+        double rd[PER], rx[PER], ry[PER];
+        if (p0 < p1) {
+            fetch_blk<PER>(BL2, dinv + (size_t)dinv_idx[lp_i[p0]] * b2, rd);
+            fetch_blk<PER>(BL2, A + (size_t)lp_aji[p0] * b2, rx);
+            fetch_blk<PER>(BL2, A + (size_t)lp_aij[p0] * b2, ry);
+        }
+        load_pad<BLC>(A + (size_t)diag_a[j] * b2, Ap);
+        for (int p = p0; p < p1; p++) {
+            stash_pad<BLC, PER>(rd, Dp);
+            stash_pad<BLC, PER>(rx, Xp);
+            stash_pad<BLC, PER>(ry, Yp);
+            __syncthreads();
+            if (p + 1 < p1) {  // next neighbour's blocks in flight during the products
+                fetch_blk<PER>(BL2, dinv + (size_t)dinv_idx[lp_i[p + 1]] * b2, rd);
+                fetch_blk<PER>(BL2, A + (size_t)lp_aji[p + 1] * b2, rx);
+                fetch_blk<PER>(BL2, A + (size_t)lp_aij[p + 1] * b2, ry);
+            }
+            gemm_pad<BLC>(Xp, Dp, Tp, false);                               // L_ji
+            gemm_pad_to_global<BLC>(Dp, Yp, Uv + (size_t)lp_u[p] * b2);     // U_ij
+            __syncthreads();
+            store_pad<BLC>(Tp, Lv + (size_t)lp_l[p] * b2);
+            gemm_pad<BLC>(Tp, Yp, Ap, true);                                // Ahat_jj -= L_ji A_ij
+            __syncthreads();
+        }
+        __syncthreads();
+        // Ahat_jj goes to its D^{-1} slot; k_block_inverse inverts it in place
+        store_pad<BLC>(Ap, dinv + (size_t)dinv_idx[j] * b2);
+        return;
+    } else if constexpr (BLC > 0) {  // compiled-in sizes not divisible by 8: scalar products
+        constexpr int PER = (BLC * BLC + FT - 1) / FT;
         double rd[PER], rx[PER], ry[PER];
         if (p0 < p1) {
             fetch_blk<PER>(BL2, dinv + (size_t)dinv_idx[lp_i[p0]] * b2, rd);
@@ -354,21 +431,13 @@ __global__ void __launch_bounds__(FT) k_ilu_factor(int bl_rt, const int *__restr
                 fetch_blk<PER>(BL2, A + (size_t)lp_aji[p + 1] * b2, rx);
                 fetch_blk<PER>(BL2, A + (size_t)lp_aij[p + 1] * b2, ry);
             }
-            if constexpr (TC) {
-                smem_gemm_dmma(BL, X, D, T, false);                           // L_ji
-                dmma_gemm_to_global(BL, D, Y, Uv + (size_t)lp_u[p] * b2);     // U_ij
-                __syncthreads();
-                store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
-                smem_gemm_dmma(BL, T, Y, Ah, true);                           // Ahat_jj -= L_ji A_ij
-            } else {
-                smem_gemm(BL, X, D, T, false);
-                __syncthreads();
-                store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
-                smem_gemm(BL, T, Y, Ah, true);
-                smem_gemm(BL, D, Y, X, false);
-                __syncthreads();
-                store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
-            }
+            smem_gemm(BL, X, D, T, false);  // L_ji
+            __syncthreads();
+            store_blk(BL, T, Lv + (size_t)lp_l[p] * b2);
+            smem_gemm(BL, T, Y, Ah, true);   // Ahat_jj -= L_ji A_ij
+            smem_gemm(BL, D, Y, X, false);   // U_ij
+            __syncthreads();
+            store_blk(BL, X, Uv + (size_t)lp_u[p] * b2);
             __syncthreads();
         }
     } else {
@@ -446,7 +515,8 @@ __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, con
 template <class TA, class TS, int BLC>
 cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
     const int BL = P->bl;
-    const size_t smem = 5 * (size_t)BL * BL * sizeof(double) + 16;
+    const int ld = (BLC > 0 && BLC % 8 == 0) ? BL + 4 : BL;  // padded blocks on the DMMA path
+    const size_t smem = 5 * (size_t)BL * ld * sizeof(double) + 16;
     if ((int)smem > 48 * 1024)  // per launch: contexts on several host threads may share the kernel
         CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS, BLC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                            (int)smem));
