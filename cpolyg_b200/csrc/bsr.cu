@@ -551,8 +551,10 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
 // order as the level form, so the same bits; same progress argument and the
 // same bounded waits.
 // ---------------------------------------------------------------------------
+// fill the SM with rows in flight: registers capped so that 1,920 threads
+// (12 CTAs of 160) fit, as rows are latency bound
 template <class T, int BL, int TPR>
-__global__ void __launch_bounds__(TPR)
+__global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
     k_sweep_direct(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
                    const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags,
                    int gen, int *counter, int *err) {
