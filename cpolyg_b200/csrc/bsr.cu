@@ -10,7 +10,8 @@
 //   FORWARD  x_i = x_i - sum_k L_k x_{c_k}           (ILU forward sweep)
 //   BACKWARD x_i = D^{-1}_i x_i - sum_k U_k x_{c_k}   (ILU backward sweep,
 //            the row's first block is D^{-1}_i; block Jacobi has only it)
-// Triangular sweeps either run sync-free (k_sweep, one launch per sweep) or
+// Triangular sweeps either run sync-free, one launch per sweep (k_sweep_direct
+// with rows streamed straight into registers, or k_sweep with a TMA ring), or
 // one launch per level of the level schedule computed from the block pattern.
 #include <algorithm>
 #include <cstdlib>
