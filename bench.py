@@ -1,13 +1,20 @@
 #!/usr/bin/env python
-"""Benchmark: DIRK3 steps/s of the 2D Euler isentropic vortex on 100,000
-periodic Voronoi cells (p=3, 40x40 blocks), FP64, GMRES(30) + block ILU(0),
-tolerance 1e-10, dt = 0.05 -- the reference's DG hot path end to end.
+"""Benchmark: 3-stage DIRK steps/s of the 2D Euler isentropic vortex on
+100,000 periodic Voronoi cells (p=3, 40x40 blocks), FP64, GMRES(30) + block
+ILU(0), tolerance 1e-10, dt = 0.05 -- the reference's DG hot path end to end.
+
+The 3-stage DIRK is Alexander's L-stable SDIRK3 by default.  The reference's
+own 3-stage tableau (getDIRK, src/TimeIntegration.cpp:70-77) is not A-stable
+(|R(-inf)| = 1.78): at this time step (CFL ~ 50 for the p=3 modes) its stiff
+modes grow every step until the state turns non-physical; --tableau
+reference selects it anyway.
 
 Arms:
   default            this library on N GPUs (one process per GPU, replicas:
                      the path does not shard, every rank runs its own solve)
   --impl reference   the reference's CPU path, i.e. the oracle restatement
-                     (oracle/), on this host's cores, on a bounded sample.
+                     (oracle/), on this host's cores, on a bounded sample;
+                     it builds its own meshes and never loads the library.
 
 Prints one JSON line on rank 0.
 """
@@ -39,6 +46,9 @@ def parse():
     ap.add_argument("--cells", type=int, default=100000)
     ap.add_argument("--degree", type=int, default=3)
     ap.add_argument("--dt", type=float, default=0.05)
+    ap.add_argument("--tableau", default="sdirk3", choices=["sdirk3", "reference"],
+                    help="3-stage DIRK tableau: Alexander's L-stable SDIRK3 (default) or the reference's getDIRK(3), "
+                         "which is not A-stable")
     ap.add_argument("--precision", default="f64", choices=["f64", "mixed", "pc32"],
                     help="f64; mixed = FP32 Jacobian and factors with FP64 FGMRES; pc32 = FP64 Jacobian with FP32 "
                          "factors (FP64 operator, FP32 preconditioner)")
@@ -93,14 +103,18 @@ def workload(a) -> dict:
                 "precision": a.precision, "jacobian": "exact", "newton_tol": a.newton_tol,
                 "newton_rtol": a.newton_rtol, "reuse_jacobian": a.reuse_jacobian,
                 "l2": "inputs larger than L2: each stage Jacobian streams ~16 GB per matvec"}
+    tab = ("Alexander's L-stable SDIRK3 (gamma 0.435866521508459; the reference's getDIRK(3) tableau is not "
+           "A-stable and diverges at this CFL)" if a.tableau == "sdirk3" else
+           "the reference's getDIRK(3) tableau (order 2, not A-stable)")
     return {"workload": f"euler-isentropic-vortex periodic [0,10]^2, {a.cells} Voronoi cells (seed 2), p={a.degree}, "
-                        f"DIRK3 dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton {a.newton_tol:g}, {prec}",
+                        f"3-stage DIRK = {tab}, dt={a.dt}, GMRES(30)+block ILU(0) tol 1e-10, Newton "
+                        f"{a.newton_tol:g}, {prec}",
             "cells": a.cells, "degree": a.degree, "block": 4 * (a.degree + 1) * (a.degree + 2) // 2,
-            "dt": a.dt, "gmres_m": 30, "gmres_tol": 1e-10, "preconditioner": "ilu0",
+            "dt": a.dt, "tableau": a.tableau, "gmres_m": 30, "gmres_tol": 1e-10, "preconditioner": "ilu0",
             "precision": a.precision, "newton_tol": a.newton_tol, "newton_rtol": a.newton_rtol,
             "reuse_jacobian": a.reuse_jacobian,
             "jacobian": "exact (the reference's A_x entry and own-state neighbour blocks corrected; same residual "
-                        "and converged solution, quadratic Newton); the CPU arm runs the reference's Jacobian",
+                        "and converged solution, quadratic Newton); the CPU arm runs the same",
             "l2": "inputs larger than L2: the Jacobian and ILU factors stream ~9 GB each per sweep"}
 
 
@@ -179,39 +193,59 @@ def profiled_traffic(name: str):
 
 
 # ------------------------------------------------------------------ CPU arm
-def cpu_sample(a, target_s: float = 12.0):
-    """Time the oracle (the reference's CPU algorithm) on a bounded sample of
-    the workload: the same problem on a smaller mesh, scaled to the full cell
-    count by the cell ratio.  Returns (steps_per_s_at_full_size, info)."""
-    import numpy as np  # noqa: F401
-
-    import cpolyg_b200 as cp
+def oracle_sample(a, n: int, threads: int, exact: bool = True):
+    """Time the oracle (the reference's CPU algorithm, restated) on one step of
+    the workload on an n-cell mesh at the workload's CFL: the time step is
+    scaled by the cell size, dt_s = dt * sqrt(cells / n), so that dt/h -- and
+    with it the Newton and GMRES iteration counts -- stay those of the full
+    problem.  The oracle builds its own seeded Voronoi mesh; nothing of the
+    library is loaded.  Returns (steps/s scaled to the full cell count, info)."""
     import oracle
-    oracle.set_threads(0)
-    threads = oracle.get_threads()
-    n = 600 if a.degree == 3 else 1500
+    oracle.set_threads(threads)
+    nthr = oracle.get_threads()
+    dt = a.dt * (a.cells / n) ** 0.5
     if a.workload == "irk":
         inflow = [1.0, 0.3, 0.0, (1.0 / GAMMA) / (GAMMA - 1) + 0.5 * 0.3 ** 2]
-        codes = [cp.BC_WALL, cp.BC_OUTFLOW, cp.BC_WALL, cp.BC_INFLOW]
-        m = cp.PolyMesh.voronoi(cp.uniform_seeds(5, n, WIDTH, WIDTH), WIDTH, WIDTH, periodic=False,
-                                side_codes=codes)
-        om = oracle.Mesh(m.export(), side_codes=codes)
-        oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=0, dparams=inflow, inflow=inflow)
+        codes = [-2, -3, -2, -4]  # wall, outflow, wall, inflow (bottom, right, top, left)
+        om = oracle.Mesh.voronoi(oracle.uniform_seeds(5, n, WIDTH, WIDTH), WIDTH, WIDTH, periodic=False,
+                                 side_codes=codes)
+        oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=0, dparams=inflow, inflow=inflow,
+                             exact_jacobian=exact)
         u = oe.interp(3, [0.1, 0.5, 5.0, 5.0, 0.3, GAMMA])
         st = oracle.Stepper(oe, 6, pc=3, gmres_m=40, gmres_tol=1e-9, gmres_maxit=20000)
     else:
-        seeds = cp.uniform_seeds(2, n, WIDTH, WIDTH)
-        m = cp.PolyMesh.voronoi(seeds, WIDTH, WIDTH, periodic=True)
-        om = oracle.Mesh(m.export())
-        oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=2, dparams=VORTEX)
+        om = oracle.Mesh.voronoi(oracle.uniform_seeds(2, n, WIDTH, WIDTH), WIDTH, WIDTH, periodic=True)
+        oe = oracle.Equation(om, 2, a.degree, gamma=GAMMA, dkind=2, dparams=VORTEX, exact_jacobian=exact)
         u = oe.interp(2, VORTEX)
-        st = oracle.Stepper(oe, 4, pc=2, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000)
+        st = oracle.Stepper(oe, 10 if a.tableau == "sdirk3" else 4, pc=2, gmres_m=30, gmres_tol=1e-10,
+                            gmres_maxit=90000)
     t0 = time.perf_counter()
-    u = st.advance(u, a.dt, 0.0)
+    u = st.advance(u, dt, 0.0)
     dt1 = time.perf_counter() - t0
-    info = {"sample_cells": n, "sample_seconds": dt1, "newton": int(st.stats[0]), "gmres": int(st.stats[1]),
-            "threads": threads}
+    info = {"cells": n, "seconds": dt1, "dt": dt, "newton": int(st.stats[0]), "gmres": int(st.stats[1]),
+            "converged": int(st.stats[3]), "threads": nthr}
     return 1.0 / (dt1 * a.cells / n), info
+
+
+# sample sizes: one step of the all-core sample takes a few seconds on 16
+# cores, the single-thread sample ~10 s
+CPU_SAMPLE_CELLS = {"dirk3": 200, "irk": 400}
+CPU_SAMPLE_CELLS_1T = {"dirk3": 100, "irk": 150}
+
+
+def describe(info, a) -> str:
+    return (f"one step of the same problem on a {info['cells']}-cell oracle mesh at the workload's CFL "
+            f"(dt {info['dt']:.3f} = dt*sqrt({a.cells}/{info['cells']})), {info['seconds']:.1f} s on "
+            f"{info['threads']} thread(s), Newton {info['newton']}, GMRES {info['gmres']}; scaled by "
+            f"{a.cells}/{info['cells']} cells")
+
+
+def cpu_baseline(a):
+    """all-core and single-thread oracle samples for the GPU arm's line"""
+    v, info = oracle_sample(a, CPU_SAMPLE_CELLS[a.workload], 0)
+    v1, info1 = oracle_sample(a, CPU_SAMPLE_CELLS_1T[a.workload], 1)
+    return {"value": v, "unit": "steps/s", "cores": info["threads"], "kind": "port", "sample": describe(info, a),
+            "value_1thread": v1, "sample_1thread": describe(info1, a)}
 
 
 def run_reference(a):
@@ -222,22 +256,26 @@ def run_reference(a):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; its per-solve "
                           "CPU cost is measured by the dirk3 and irk workloads"}), flush=True)
         return
-    vals = []
-    info = None
+    vals, info = [], None
     for k in range(a.warmup + a.steps):
-        v, info = cpu_sample(a)
+        v, info = oracle_sample(a, CPU_SAMPLE_CELLS[a.workload], 0)
         if k >= a.warmup:
             vals.append(v)
     value = sum(vals) / len(vals)
-    sample = (f"one DIRK3 step of the same problem on a {info['sample_cells']}-cell mesh "
-              f"({info['sample_seconds']:.1f} s, Newton {info['newton']}, GMRES {info['gmres']} its), "
-              f"scaled by {a.cells}/{info['sample_cells']} cells")
+    v1, info1 = oracle_sample(a, CPU_SAMPLE_CELLS_1T[a.workload], 1)
+    # the reference's own (inexact) Euler Jacobian on the all-core sample:
+    # same converged solution, linearly converging Newton
+    vr, infor = oracle_sample(a, CPU_SAMPLE_CELLS[a.workload], 0, exact=False)
     out = {"metric": METRIC, "value": value, "unit": "steps/s", "impl": "reference", "n_gpus": a.gpus,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Voronoi mesh)",
            "config": workload(a),
            "cpu_baseline": {"value": value, "unit": "steps/s", "cores": info["threads"], "kind": "port",
-                            "sample": sample},
+                            "sample": describe(info, a) + f"; mean of {a.steps} samples after {a.warmup}",
+                            "value_1thread": v1, "sample_1thread": describe(info1, a),
+                            "value_reference_jacobian": vr,
+                            "sample_reference_jacobian": describe(infor, a) + " (the reference's inexact Euler "
+                            f"Jacobian, Newton converged: {bool(infor['converged'])})"},
            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
 
@@ -269,8 +307,8 @@ def build_problem(a, cp, ctx):
 
     def make(mixed):
         m32 = mixed == "mixed"
-        return cp.DIRK(3, eq, pc=cp.PC_ILU0, precision=cp.F32 if m32 else cp.F64, gmres_m=30, gmres_tol=1e-10,
-                       gmres_maxit=90000, flexible=m32, newton_tol=a.newton_tol,
+        return cp.DIRK(3, eq, l_stable=a.tableau == "sdirk3", pc=cp.PC_ILU0, precision=cp.F32 if m32 else cp.F64,
+                       gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000, flexible=m32, newton_tol=a.newton_tol,
                        reuse_jacobian=a.reuse_jacobian, newton_rtol=a.newton_rtol, pc_f32=mixed == "pc32")
     return eq, make, u0
 
@@ -342,6 +380,76 @@ def run_serve(a):
         dist.destroy_process_group()
 
 
+def _timed(fn, reps, stream):
+    """device time per call of fn (CUDA events on the launching stream)"""
+    import torch
+    for _ in range(2):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps / 1000.0
+
+
+def roofline(a, cp, ctx, eq, u, t, stream):
+    """ILU(0) apply (two sync-free sweep launches) and BSR matvec of the
+    step's Newton matrix B = M - gamma dt J at the current state, each
+    against the measured HBM copy bandwidth.  Algorithmic bytes:
+    sweeps nnzb*bl^2*s + 4*n*bl*8 (every factor block once; forward and
+    backward read and write the vector), matvec nnzb*bl^2*s + 2*n*bl*8."""
+    import torch
+    if a.workload != "dirk3":
+        return None
+    mixed = a.precision == "mixed"
+    s_a = 4 if mixed else 8
+    s_p = 4 if a.precision in ("mixed", "pc32") else 8
+    gamma = 0.435866521508459 if a.tableau == "sdirk3" else 0.717933260754229
+    J = eq.jacobian(u, t, scale=-a.dt * gamma, add_mass=True, precision=cp.F32 if mixed else cp.F64)
+    P = cp.BlockILU0(J, precision=cp.F32 if s_p == 4 else cp.F64)
+    x = torch.randn(u.numel(), dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    n, bl, nnzb = J.n_rows, J.bl, J.nb
+    pk = peaks()
+    reps = 20
+    ctx.check(ctx._lib.cpg_ctx_set_deferred_checks(ctx.h, 1))  # no host read-back between the launches
+    try:
+        torch.cuda.nvtx.range_push("roofline_sweep")
+        t_sw = _timed(lambda: ctx.check(ctx._lib.cpg_precond_apply(ctx.h, P.h, cp.C.c_void_p(x.data_ptr()))),
+                      reps, stream)
+        torch.cuda.nvtx.range_pop()
+        ctx.sync()  # reads the sweeps' status word
+        torch.cuda.nvtx.range_push("roofline_matvec")
+        t_mv = _timed(lambda: ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()),
+                                                                cp.C.c_void_p(y.data_ptr()))), reps, stream)
+        torch.cuda.nvtx.range_pop()
+    finally:
+        ctx.check(ctx._lib.cpg_ctx_set_deferred_checks(ctx.h, 0))
+    form = int(ctx._lib.cpg_precond_sweep_form(P.h))
+    alg_sw = nnzb * bl * bl * s_p + 4 * n * bl * 8
+    alg_mv = nnzb * bl * bl * s_a + 2 * n * bl * 8
+    ach_sw, ach_mv = alg_sw / t_sw / 1e9, alg_mv / t_mv / 1e9
+    prec_sw = "FP32" if s_p == 4 else "FP64"
+    kname = {1: "k_sweep (TMA ring)", 4: "k_sweep_direct", 5: "k_sweep_direct (2x rows)",
+             6: "k_sweep_direct (4x rows)", 2: "k_rows per level", 3: "k_rows per level (wide)"}.get(form, "sweep")
+    traffic = profiled_traffic(f"sweep_direct_{prec_sw.lower()}_bl{bl}_100k.md")
+    roof = {"kernel": f"{kname}: ILU(0) apply, forward + backward sweep, {bl}x{bl} {prec_sw} factors "
+                      f"(sweep form {form})",
+            "bound": "hbm", "achieved": ach_sw, "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": ach_sw / pk["hbm_gbs"], "peak_source": pk["source"], "algorithmic_bytes": alg_sw,
+            "launch_ms": t_sw * 1e3, "launches_per_unit": 2 if form in (1, 4, 5, 6) else None,
+            "traffic": traffic,
+            "matvec": {"kernel": f"k_rows (BSR matvec, {bl}x{bl} {'FP32' if mixed else 'FP64'} blocks)",
+                       "achieved": ach_mv, "frac": ach_mv / pk["hbm_gbs"], "algorithmic_bytes": alg_mv,
+                       "launch_ms": t_mv * 1e3,
+                       "traffic": profiled_traffic(f"bsr_matvec_{'f32' if mixed else 'f64'}_bl{bl}.md")}}
+    del P, J
+    return roof
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -391,14 +499,14 @@ def run_ours(a):
     clocks.start()
     time.sleep(0.3)
     launches0 = ctx.launches
-    newton = gmres = 0
+    newton, gmres = [], []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
     for _ in range(a.steps):
         stepper.advance(u, a.dt, t)
-        newton += stepper.stats.newton_iterations
-        gmres += stepper.stats.gmres_iterations
+        newton.append(stepper.stats.newton_iterations)
+        gmres.append(stepper.stats.gmres_iterations)
         t += a.dt
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -426,46 +534,16 @@ def run_ours(a):
         e2e = {"value": world * a.steps / float(e2e_s.item()), "unit": "steps/s",
                "h2d_bytes_per_step": int(uh.nbytes), "d2h_bytes_per_step": int(uh.nbytes)}
 
-    # roofline of the dominant kernel class (block-row streaming kernel:
-    # BSR matvec), timed live with CUDA events on the launching stream
+    # roofline of the dominant kernel: the ILU(0) triangular sweeps (one
+    # forward and one backward launch per application, ~40% of the step),
+    # then the BSR matvec (~38%); both timed live with CUDA events on the
+    # launching stream, on the step's own Newton matrix and its factors
     roof = None
     if rank == 0:
-        J = eq.jacobian(u, t, scale=-a.dt * 0.717933260754, add_mass=True,
-                        precision=cp.F32 if mixed else cp.F64)
-        x = torch.randn(u.numel(), dtype=torch.float64, device="cuda")
-        y = torch.empty_like(x)
-        for _ in range(3):
-            ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())))
-        reps = 20
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.nvtx.range_push("roofline_matvec")  # lets ncu select exactly these launches
-        e0.record(stream)
-        for _ in range(reps):
-            ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())))
-        e1.record(stream)
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
-        t_launch = e0.elapsed_time(e1) / reps / 1000.0
-        s_a = 4 if mixed else 8
-        alg = J.nb * J.bl * J.bl * s_a + 2 * J.n_rows * J.bl * 8
-        pk = peaks()
-        ach = alg / t_launch / 1e9
-        traffic = profiled_traffic(f"bsr_matvec_{'f32' if mixed else 'f64'}_bl{J.bl}.md")
-        roof = {"kernel": f"k_rows (BSR matvec, {J.bl}x{J.bl} {'FP32' if mixed else 'FP64'} blocks)",
-                "bound": "hbm", "achieved": ach,
-                "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
-                "peak_source": pk["source"], "algorithmic_bytes": alg, "launch_ms": t_launch * 1e3,
-                "traffic": traffic}
-        del J
+        roof = roofline(a, cp, ctx, eq, u, t, stream)
 
     if rank == 0:
-        cpu = None
-        if not a.no_cpu_baseline and world == 1:
-            v, info = cpu_sample(a)
-            cpu = {"value": v, "unit": "steps/s", "cores": info["threads"], "kind": "port",
-                   "sample": (f"oracle step on a {info['sample_cells']}-cell mesh of the same problem "
-                              f"({info['sample_seconds']:.1f} s, Newton {info['newton']}, GMRES {info['gmres']} "
-                              f"its), scaled by cell count")}
+        cpu = cpu_baseline(a) if (not a.no_cpu_baseline and world == 1) else None
         out = {"metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None,
@@ -473,7 +551,8 @@ def run_ours(a):
                    a.precision, "f64"),
                "data": "synthetic (seeded Voronoi mesh, analytic initial data)",
                "config": dict(workload(a), parallelism=f"replicas x{world}"),
-               "newton_iterations_per_step": newton / a.steps, "gmres_iterations_per_step": gmres / a.steps,
+               "newton_iterations_per_step": sum(newton) / a.steps, "gmres_iterations_per_step": sum(gmres) / a.steps,
+               "newton_per_step": newton, "gmres_per_step": gmres,
                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk}
         if err_fp64 is not None:
             out["error_vs_fp64"] = {"value": err_fp64, "steps": a.compare_fp64,

@@ -19,12 +19,12 @@ from . import _capi
 from ._capi import (ADVECTION_CONST, ADVECTION_ROTATING, BC_DIRICHLET, BC_INFLOW, BC_OUTFLOW, BC_WALL, EULER, F32,
                     F64, INIT_CONSTANT, INIT_DENSITY_BUMP, INIT_GAUSSIAN, INIT_VORTEX, PC_BJACOBI, PC_ILU0, PC_NONE,
                     PC_STAGE_BJACOBI, STEP_BACKWARD_EULER, STEP_DIRK3, STEP_DIRK5, STEP_FORWARD_EULER, STEP_IRK2,
-                    STEP_IRK2_INV, STEP_IRK3, STEP_IRK3_INV, STEP_RK2, STEP_RK4, CpgError)
+                    STEP_IRK2_INV, STEP_IRK3, STEP_IRK3_INV, STEP_RK2, STEP_RK4, STEP_SDIRK3, CpgError)
 
 __all__ = [
     "lib", "Context", "PolyMesh", "Equation", "Advection", "ConstantAdvection", "Euler", "BlockMatrix",
     "Jacobian", "NoPreconditioner", "BlockJacobi", "BlockILU0", "TimeStepper", "ForwardEuler", "RK2", "RK4",
-    "BackwardEuler", "DIRK", "IRK", "CpgError",
+    "BackwardEuler", "DIRK", "SDIRK3", "IRK", "CpgError",
 ]
 
 
@@ -486,9 +486,21 @@ class BackwardEuler(TimeStepper):
 
 
 class DIRK(TimeStepper):
-    def __init__(self, nStages: int, eq: Equation, **kw):
-        self.kind = {3: STEP_DIRK3, 5: STEP_DIRK5}[nStages]
+    """DIRK::advance (src/TimeIntegration.cpp:93-151).  nStages = 3 is the
+    reference's tableau (getDIRK, :70-77: order 2, not A-stable); pass
+    l_stable=True for Alexander's L-stable SDIRK3 (same as SDIRK3)."""
+
+    def __init__(self, nStages: int, eq: Equation, l_stable: bool = False, **kw):
+        if l_stable and nStages != 3:
+            raise ValueError("the L-stable tableau has 3 stages")
+        self.kind = STEP_SDIRK3 if l_stable else {3: STEP_DIRK3, 5: STEP_DIRK5}[nStages]
         super().__init__(eq, **kw)
+
+
+class SDIRK3(TimeStepper):
+    """Alexander's L-stable 3-stage SDIRK of order 3 on the DIRK::advance
+    Newton/GMRES path (the reference's DIRK3 with an A-stable tableau)."""
+    kind = STEP_SDIRK3
 
 
 class IRK(TimeStepper):

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libcpolyg_b200.so")
 STATUS = {
     0: "CPG_OK", 1: "CPG_ERR_INVALID_ARG", 2: "CPG_ERR_OOM", 3: "CPG_ERR_SINGULAR_BLOCK",
     4: "CPG_ERR_NONFINITE", 5: "CPG_ERR_NOT_CONVERGED", 6: "CPG_ERR_TIMEOUT", 7: "CPG_ERR_CUDA",
-    8: "CPG_ERR_MESH", 9: "CPG_ERR_UNSUPPORTED",
+    8: "CPG_ERR_MESH", 9: "CPG_ERR_UNSUPPORTED", 10: "CPG_ERR_NONPHYSICAL",
 }
 
 # enums (cpolyg.h)
@@ -24,7 +24,7 @@ INIT_CONSTANT, INIT_GAUSSIAN, INIT_VORTEX, INIT_DENSITY_BUMP = 0, 1, 2, 3
 F64, F32 = 0, 1
 PC_NONE, PC_BJACOBI, PC_ILU0, PC_STAGE_BJACOBI = 0, 1, 2, 3
 (STEP_FORWARD_EULER, STEP_RK2, STEP_RK4, STEP_BACKWARD_EULER, STEP_DIRK3, STEP_DIRK5,
- STEP_IRK2, STEP_IRK3, STEP_IRK2_INV, STEP_IRK3_INV) = range(10)
+ STEP_IRK2, STEP_IRK3, STEP_IRK2_INV, STEP_IRK3_INV, STEP_SDIRK3) = range(11)
 
 
 class MeshInfo(C.Structure):
@@ -75,6 +75,7 @@ PROTOTYPES = {
     "cpg_ctx_destroy": (None, [P]),
     "cpg_last_error": (C.c_char_p, [P]),
     "cpg_ctx_sync": (I, [P]),
+    "cpg_ctx_set_deferred_checks": (I, [P, I]),
     "cpg_ctx_launch_count": (C.c_uint64, [P]),
     "cpg_version": (C.c_char_p, []),
     "cpg_seeds_uniform": (I, [C.c_uint64, I, D, D, PD]),

@@ -23,6 +23,9 @@ struct cpg_ctx {
     double *pinned = nullptr;
     size_t pinned_cap = 0;
     int *flag_dev = nullptr;  // device status word (singular pivots etc.)
+    // 1: cpg_precond_apply and cpg_assemble leave their device status words
+    // to the next cpg_ctx_sync instead of synchronizing to read them
+    int deferred_checks = 0;
     // grow-only Krylov workspace (basis vectors), kept across solves
     double *kws = nullptr;
     size_t kws_cap = 0;  // doubles
@@ -37,6 +40,12 @@ cpg_status scratch(cpg_ctx *ctx, size_t n, double **out);
 cpg_status pinned(cpg_ctx *ctx, size_t n, double **out);
 // check the last launch; increments the launch counter
 cpg_status launched(cpg_ctx *ctx, const char *what);
+// slot of ctx->flag_dev where the residual kernel records the first cell
+// (+1) whose state is not admissible (0 = none)
+constexpr int FLAG_NONPHYS = 8;
+// synchronizes the context's stream, then reads and clears that slot:
+// CPG_ERR_NONPHYSICAL naming the cell and `where` if it was set
+cpg_status check_state(cpg_ctx *ctx, const std::string &where);
 
 template <class T>
 cpg_status dmalloc(cpg_ctx *ctx, T **p, size_t n) {

@@ -3,6 +3,7 @@
 #include <new>
 
 #include "common.cuh"
+#include "internal.hpp"
 #include "mesh.hpp"
 
 struct cpg_mesh {
@@ -61,6 +62,21 @@ cpg_status launched(cpg_ctx *ctx, const char *what) {
     return CPG_OK;
 }
 
+cpg_status check_state(cpg_ctx *ctx, const std::string &where) {
+    double *hp;
+    CPG_TRY(pinned(ctx, 1, &hp));
+    int *flag = (int *)hp;
+    CPG_CUDA(ctx, cudaMemcpyAsync(flag, ctx->flag_dev + FLAG_NONPHYS, sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream));
+    CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const int v = *flag;
+    if (v == 0) return CPG_OK;
+    CPG_CUDA(ctx, cudaMemsetAsync(ctx->flag_dev + FLAG_NONPHYS, 0, sizeof(int), ctx->stream));
+    return fail(ctx, CPG_ERR_NONPHYSICAL,
+                "non-physical state (density or pressure <= 0, or not finite) in cell " + std::to_string(v - 1) +
+                    " (" + where + ")");
+}
+
 }  // namespace cpg
 
 using namespace cpg;
@@ -110,6 +126,13 @@ const char *cpg_last_error(const cpg_ctx *ctx) { return ctx ? ctx->err.c_str() :
 cpg_status cpg_ctx_sync(cpg_ctx *ctx) {
     if (!ctx) return CPG_ERR_INVALID_ARG;
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    CPG_TRY(check_sweep_error(ctx, CPG_OK));
+    return check_state(ctx, "a residual since the last check");
+}
+
+cpg_status cpg_ctx_set_deferred_checks(cpg_ctx *ctx, int on) {
+    if (!ctx) return CPG_ERR_INVALID_ARG;
+    ctx->deferred_checks = on != 0;
     return CPG_OK;
 }
 

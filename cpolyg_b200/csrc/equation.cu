@@ -24,9 +24,12 @@ constexpr int nqf_of(int p) { return (2 * p <= 2) ? 2 : ((2 * p <= 4) ? 4 : 6); 
 // contracted against every test function (the reference recomputes them per
 // test function, Equation.cpp:176-187).
 // ---------------------------------------------------------------------------
+// A state that is not admissible (Euler: density or pressure <= 0, or not
+// finite) at any of the cell's quadrature points records the cell in
+// *nonphys (cell + 1, first writer wins) for the host to report.
 template <class Phys, int P>
 __global__ void __launch_bounds__(128) k_residual(Geo g, Phys ph, BCParams bc, const double *__restrict__ u,
-                                                  double t, double *__restrict__ b) {
+                                                  double t, double *__restrict__ b, int *__restrict__ nonphys) {
     constexpr int NB = nbasis<P>(), NC = Phys::NC, BL = NB * NC, NQF = nqf_of(P);
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     const int cell = blockIdx.x * (blockDim.x >> 5) + wid;
@@ -40,6 +43,7 @@ __global__ void __launch_bounds__(128) k_residual(Geo g, Phys ph, BCParams bc, c
     double acc[BL];
 #pragma unroll
     for (int r = 0; r < BL; r++) acc[r] = 0.0;
+    bool bad = false;
 
     const int q1 = g.vq_ptr[cell + 1];
     for (int q = g.vq_ptr[cell] + lane; q < q1; q += 32) {
@@ -53,6 +57,7 @@ __global__ void __launch_bounds__(128) k_residual(Geo g, Phys ph, BCParams bc, c
             for (int k = 0; k < NB; k++) s += U[c * NB + k] * psi[k];
             uu[c] = s;
         }
+        bad |= !ph.admissible(uu);
         double Fx[NC], Fy[NC];
         ph.flux(uu, g.vx[q], g.vy[q], Fx, Fy);
         const double w = g.vw[q];
@@ -77,6 +82,7 @@ __global__ void __launch_bounds__(128) k_residual(Geo g, Phys ph, BCParams bc, c
             for (int k = 0; k < NB; k++) s += U[c * NB + k] * psi[k];
             um[c] = s;
         }
+        bad |= !ph.admissible(um);
         const int nbr = g.f_nbr[f];
         const double nx = g.f_nx[f], ny = g.f_ny[f], x = g.qx[fq], y = g.qy[fq];
         if (nbr >= 0) {
@@ -113,6 +119,7 @@ __global__ void __launch_bounds__(128) k_residual(Geo g, Phys ph, BCParams bc, c
 #pragma unroll
     for (int r = 0; r < BL; r++)
         if ((r & 31) == lane) b[(size_t)cell * BL + r] = acc[r];
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicCAS(nonphys, 0, cell + 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -764,15 +771,19 @@ cpg_status cpg_equation_get_info(const cpg_equation *eq, cpg_equation_info *info
     return CPG_OK;
 }
 
+// Equation::assemble (Equation.cpp:152-191) as seen from the C ABI: the
+// residual, then -- outside stream capture -- a read of the state word, so
+// that a non-physical state is reported by the call that met it.  The
+// steppers launch the kernel alone (assemble_raw) and read the word at the
+// synchronisation their Newton norms make anyway.
 cpg_status cpg_assemble(cpg_ctx *ctx, const cpg_equation *eq, const double *u, double t, double *b) {
     if (!ctx || !eq || !u || !b) return CPG_ERR_INVALID_ARG;
-    return with_physics(eq, [&](auto ph, auto pc) -> cpg_status {
-        constexpr int P = decltype(pc)::value;
-        const int cells_per_cta = 4;
-        const int grid = (eq->n + cells_per_cta - 1) / cells_per_cta;
-        k_residual<decltype(ph), P><<<grid, 32 * cells_per_cta, 0, ctx->stream>>>(eq->geo(), ph, eq->bc, u, t, b);
-        return launched(ctx, "residual kernel");
-    });
+    CPG_TRY(assemble_raw(ctx, eq, u, t, b));
+    if (ctx->deferred_checks) return CPG_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CPG_CUDA(ctx, cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return CPG_OK;
+    return check_state(ctx, "residual");
 }
 
 cpg_status cpg_jacobian(cpg_ctx *ctx, const cpg_equation *eq, const double *u, double t, double scale, int add_mass,
@@ -943,6 +954,16 @@ extern "C" cpg_status cpg_l2norm_noalloc(cpg_ctx *ctx, const cpg_equation *eq, c
 }
 
 namespace cpg {
+cpg_status assemble_raw(cpg_ctx *ctx, const cpg_equation *eq, const double *u, double t, double *b) {
+    return with_physics(eq, [&](auto ph, auto pc) -> cpg_status {
+        constexpr int P = decltype(pc)::value;
+        const int cells_per_cta = 4;
+        const int grid = (eq->n + cells_per_cta - 1) / cells_per_cta;
+        k_residual<decltype(ph), P><<<grid, 32 * cells_per_cta, 0, ctx->stream>>>(eq->geo(), ph, eq->bc, u, t, b,
+                                                                                  ctx->flag_dev + FLAG_NONPHYS);
+        return launched(ctx, "residual kernel");
+    });
+}
 // y = alpha * M x + beta * z (Newton residual r = M k - dt b)
 cpg_status mass_apply_axpy(cpg_ctx *ctx, const cpg_equation *eq, const double *x, double alpha, const double *z,
                            double beta, double *y) {

@@ -113,6 +113,8 @@ struct LinOp {
 };
 cpg_status gmres_op(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, double *x, int m, double tol,
                     int maxit, int flexible, cpg_solve_stats *stats);
+// residual kernel alone, without the state check of cpg_assemble (equation.cu)
+cpg_status assemble_raw(cpg_ctx *ctx, const cpg_equation *eq, const double *u, double t, double *b);
 // mass helpers (equation.cu)
 cpg_status mass_apply_axpy(cpg_ctx *ctx, const cpg_equation *eq, const double *x, double alpha, const double *z,
                            double beta, double *y);

@@ -89,6 +89,8 @@ struct Advection {
         const double bn = nx * betaX(x, y) + ny * betaY(x, y);
         J[0] = (sgn * bn > 0) ? bn : 0.0;
     }
+    // every finite scalar is an admissible state
+    __device__ __forceinline__ bool admissible(const double *U) const { return true; }
     __device__ __forceinline__ void wall(const double *Um, double nx, double ny, double *Up) const { Up[0] = Um[0]; }
     __device__ __forceinline__ void wall_deriv(double nx, double ny, double *R) const { R[0] = 1.0; }
 };
@@ -128,8 +130,12 @@ struct Euler {
         eflux(Um, fxm, fym, cm, um, vm);
         eflux(Up, fxp, fyp, cp, up, vp);
         const double vnm = um * nx + vm * ny, vnp = up * nx + vp * ny;
+        // fmax returns its other operand for a NaN one, so a NaN sound speed
+        // (negative pressure) would vanish from alpha; adding 0*(cm+cp)
+        // carries it into the flux and leaves every finite alpha unchanged
         const double alpha = fmax(fmax(fmax(fabs(vnm - cm), fabs(vnm)), fmax(fabs(vnm + cm), fabs(vnp - cp))),
-                                  fmax(fabs(vnp), fabs(vnp + cp)));
+                                  fmax(fabs(vnp), fabs(vnp + cp))) +
+                             0.0 * (cm + cp);
 #pragma unroll
         for (int k = 0; k < 4; k++)
             F[k] = 0.5 * ((fxp[k] + fxm[k]) * nx + (fyp[k] + fym[k]) * ny + alpha * (Um[k] - Up[k]));
@@ -213,6 +219,12 @@ struct Euler {
             for (int c = 0; c < 4; c++)
                 J[r * 4 + c] = 0.5 * (A0[r * 4 + c] * nx + A1[r * 4 + c] * ny + (r == c ? sgn * alpha : 0.0) +
                                       (U[r] - U2[r]) * ap[c]);
+    }
+    // positive density and pressure (false for NaN as well)
+    __device__ __forceinline__ bool admissible(const double *U) const {
+        const double rho = U[0];
+        const double P = (gamma - 1) * (U[3] - 0.5 * (U[1] * U[1] + U[2] * U[2]) / rho);
+        return rho > 0.0 && P > 0.0 && P < INFINITY;
     }
     __device__ __forceinline__ void wall(const double *Um, double nx, double ny, double *Up) const {
         const double mn = Um[1] * nx + Um[2] * ny;

@@ -627,9 +627,11 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     bool timed = cudaMalloc(&tmp, N * sizeof(double)) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
                  cudaEventCreate(&e1) == cudaSuccess;
     float best_ms[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+    bool dropped[6] = {false, false, false, false, false, false};
     cpg_status st = CPG_OK;
     for (int rep = 0; rep < 2 && timed && st == CPG_OK; rep++)
         for (int c = 0; c < P->n_cand && st == CPG_OK; c++) {
+            if (dropped[c]) continue;
             float ms = 1e30f;
             if (cudaMemcpyAsync(tmp, x, N * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream) != cudaSuccess ||
                 cudaEventRecord(e0, ctx->stream) != cudaSuccess) {
@@ -640,19 +642,31 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
             if (st == CPG_OK && cudaEventRecord(e1, ctx->stream) == cudaSuccess &&
                 cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
                 best_ms[c] = std::min(best_ms[c], ms);
+            // a candidate whose bounded wait ran out (e.g. other work held its
+            // SMs) is dropped; its status word must not fail the caller's solve
+            if (st == CPG_OK && check_sweep_error(ctx, CPG_OK) != CPG_OK) {
+                dropped[c] = true;
+                best_ms[c] = 1e30f;
+            }
         }
     (void)cudaGetLastError();
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (tmp) cudaFree(tmp);
     if (st != CPG_OK) return st;
-    int best = 0;
-    for (int c = 1; c < P->n_cand; c++)
-        if (best_ms[c] < best_ms[best]) best = c;
+    int best = -1;
+    for (int c = 0; c < P->n_cand; c++)
+        if (!dropped[c] && best_ms[c] < 1e29f && (best < 0 || best_ms[c] < best_ms[best])) best = c;
+    if (!timed || best < 0) {
+        // nothing was timed (no scratch memory for the copy, or every
+        // candidate gave up): apply the level form this once and decide at a
+        // later application rather than record an untimed choice
+        return apply_form(ctx, P, x, 2);
+    }
     {
         std::lock_guard<std::mutex> lk(g_form_mu);
         auto it = g_form.find(P->form_key);
-        if (it == g_form.end()) g_form[P->form_key] = timed ? P->cand[best] : 2;
+        if (it == g_form.end()) g_form[P->form_key] = P->cand[best];
         P->sweep_mode = g_form[P->form_key];  // a concurrent first decision wins
     }
     return apply_form(ctx, P, x, P->sweep_mode);
@@ -903,7 +917,9 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A) 
 
 cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     if (!ctx || !x) return CPG_ERR_INVALID_ARG;
-    return check_sweep_error(ctx, precond_apply_raw(ctx, P, x));
+    const cpg_status st = precond_apply_raw(ctx, P, x);
+    if (ctx->deferred_checks) return st;
+    return check_sweep_error(ctx, st);
 }
 
 int cpg_precond_sweep_form(const cpg_precond *P) {

@@ -126,6 +126,18 @@ void tableau(int kind, int &s, std::vector<double> &A, std::vector<double> &Ainv
             c = {(1 + alpha) / 2.0, 1.0 / 2.0, (1 - alpha) / 2.0};
             break;
         }
+        case CPG_STEP_SDIRK3: {
+            // Alexander's L-stable SDIRK of order 3 (SIAM J. Numer. Anal. 14,
+            // 1977): gamma solves g^3 - 3g^2 + 3g/2 - 1/6 = 0 in (1/6, 1/2);
+            // the last row of A is b
+            const double g = 0.435866521508459, t2 = (1 + g) / 2.0;
+            const double b1 = -(6 * g * g - 16 * g + 1) / 4.0, b2 = (6 * g * g - 20 * g + 5) / 4.0;
+            s = 3;
+            A = {g, 0, 0, t2 - g, g, 0, b1, b2, g};
+            b = {b1, b2, g};
+            c = {g, t2, 1.0};
+            break;
+        }
         case CPG_STEP_DIRK5: {  // Cooper and Sayfy, TimeIntegration.cpp:78-88
             const double g = (6 - r6) / 10.0;
             s = 5;
@@ -340,7 +352,7 @@ cpg_status newton_norm(cpg_stepper *S, const double *r, double *out) {
 
 // k = dt * M^{-1} assemble(u, t)
 cpg_status rk_stage(cpg_stepper *S, const double *u, double t, double dt, double *k) {
-    CPG_TRY(cpg_assemble(S->ctx, S->eq, u, t, S->rhs));
+    CPG_TRY(assemble_raw(S->ctx, S->eq, u, t, S->rhs));
     return mass_solve_scaled(S->ctx, S->eq, S->rhs, dt, k);
 }
 
@@ -455,10 +467,12 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
             }
             k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu);
             CPG_TRY(launched(ctx, "stage combine kernel"));
-            CPG_TRY(cpg_assemble(ctx, S->eq, S->cu, ts, S->rhs));
+            CPG_TRY(assemble_raw(ctx, S->eq, S->cu, ts, S->rhs));
             CPG_TRY(mass_apply_axpy(ctx, S->eq, ks, 1.0, S->rhs, -dt, S->r));  // r = M k - dt rhs
             double nr;
             CPG_TRY(newton_norm(S, S->r, &nr));
+            CPG_TRY(check_state(ctx, "DIRK stage " + std::to_string(stage) + ", Newton iteration " +
+                                         std::to_string(iter) + ", t = " + std::to_string(ts)));
             st->last_newton_residual = nr;
             if (nr < S->d.newton_tol && (S->d.newton_rtol <= 0 || upd_rel < S->d.newton_rtol)) break;
             st->newton_iterations++;
@@ -528,7 +542,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                 k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, nullptr, cb, S->tmp);
                 CPG_TRY(launched(ctx, "stage combine kernel"));
                 CPG_TRY(combine(S, u, {{K + i * N, 1.0}}, S->cu));  // u + w_i
-                CPG_TRY(cpg_assemble(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
+                CPG_TRY(assemble_raw(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
                 CPG_TRY(mass_apply_axpy(ctx, S->eq, S->tmp, 1.0, S->rhs, -dt, R + i * N));
                 double nr;
                 CPG_TRY(newton_norm(S, R + i * N, &nr));
@@ -544,7 +558,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                 }
                 k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu);
                 CPG_TRY(launched(ctx, "stage combine kernel"));
-                CPG_TRY(cpg_assemble(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
+                CPG_TRY(assemble_raw(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
                 CPG_TRY(mass_apply_axpy(ctx, S->eq, K + i * N, 1.0, S->rhs, -dt, R + i * N));
                 double nr;
                 CPG_TRY(newton_norm(S, R + i * N, &nr));
@@ -552,6 +566,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
             }
         }
         rNorm = std::sqrt(rNorm);
+        CPG_TRY(check_state(ctx, "implicit RK Newton iteration " + std::to_string(iter) + ", t = " + std::to_string(t)));
         st->last_newton_residual = rNorm;
         if (rNorm < S->d.newton_tol && (S->d.newton_rtol <= 0 || upd_rel < S->d.newton_rtol)) break;
         st->newton_iterations++;
@@ -647,7 +662,7 @@ extern "C" {
 
 cpg_status cpg_stepper_create(cpg_ctx *ctx, cpg_equation *eq, const cpg_stepper_desc *d, cpg_stepper **out) {
     if (!ctx || !eq || !d || !out) return CPG_ERR_INVALID_ARG;
-    if (d->kind < CPG_STEP_FORWARD_EULER || d->kind > CPG_STEP_IRK3_INV)
+    if (d->kind < CPG_STEP_FORWARD_EULER || d->kind > CPG_STEP_SDIRK3)
         return fail(ctx, CPG_ERR_INVALID_ARG, "unknown stepper kind");
     *out = nullptr;
     cpg_stepper *S = new (std::nothrow) cpg_stepper();
@@ -781,6 +796,8 @@ cpg_status cpg_step_host(cpg_ctx *ctx, cpg_stepper *S, double *u_host, double dt
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "device to host copy");
     }
     cudaStreamSynchronize(ctx->stream);
+    // explicit steps launch without a host check; the state word is read here
+    if (rc == CPG_OK) rc = check_state(ctx, "step from t = " + std::to_string(t));
     return rc;
 }
 

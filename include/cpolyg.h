@@ -48,7 +48,10 @@ typedef enum {
     CPG_ERR_TIMEOUT = 6,        /* a bounded device wait ran out            */
     CPG_ERR_CUDA = 7,           /* a CUDA runtime call failed               */
     CPG_ERR_MESH = 8,           /* inconsistent or too coarse mesh          */
-    CPG_ERR_UNSUPPORTED = 9     /* degree / block size not compiled in     */
+    CPG_ERR_UNSUPPORTED = 9,    /* degree / block size not compiled in     */
+    CPG_ERR_NONPHYSICAL = 10    /* Euler state with density or pressure
+                                   <= 0 (or not finite) at a quadrature
+                                   point; cpg_last_error names the cell     */
 } cpg_status;
 
 /* physics, replaces the four pure virtuals of Equation (src/Equation.h:46-51)
@@ -107,7 +110,15 @@ typedef enum {
     CPG_STEP_IRK2 = 6,        /* Radau IIA, 2 stages, IRK::advance           */
     CPG_STEP_IRK3 = 7,        /* Radau IIA, 3 stages, IRK::advance           */
     CPG_STEP_IRK2_INV = 8,    /* IRK::newAdvance, 2 stages                   */
-    CPG_STEP_IRK3_INV = 9     /* IRK::newAdvance, 3 stages                   */
+    CPG_STEP_IRK3_INV = 9,    /* IRK::newAdvance, 3 stages                   */
+    CPG_STEP_SDIRK3 = 10      /* DIRK::advance with Alexander's L-stable
+                                 3-stage SDIRK of order 3 (gamma =
+                                 0.435866521508459, stiffly accurate).  The
+                                 reference's getDIRK(3) (TimeIntegration.cpp:
+                                 70-77, CPG_STEP_DIRK3 here) combines this
+                                 gamma with Crouzeix's tableau: order 2 and
+                                 not A-stable (|R(-inf)| = 1.78), so stiff DG
+                                 modes grow at large time steps.             */
 } cpg_step_kind;
 
 typedef struct cpg_ctx cpg_ctx;
@@ -124,7 +135,16 @@ typedef struct cpg_stepper cpg_stepper;
 cpg_status cpg_ctx_create(int device, void *stream, cpg_ctx **out);
 void cpg_ctx_destroy(cpg_ctx *ctx);
 const char *cpg_last_error(const cpg_ctx *ctx);
+/* Waits for the context's stream, then reads the device status words that
+ * deferred calls left: a sweep whose bounded wait ran out (CPG_ERR_TIMEOUT),
+ * a residual that met a non-physical state (CPG_ERR_NONPHYSICAL).          */
 cpg_status cpg_ctx_sync(cpg_ctx *ctx);
+/* on != 0: cpg_precond_apply and cpg_assemble launch their kernels and
+ * return without synchronizing to read their status words (which they do
+ * by default), so that back-to-back calls stay asynchronous; the words are
+ * read by the next cpg_ctx_sync.  No counterpart in the reference (its calls
+ * are synchronous CPU code).                                                */
+cpg_status cpg_ctx_set_deferred_checks(cpg_ctx *ctx, int on);
 /* number of kernels this library launched on ctx since creation */
 uint64_t cpg_ctx_launch_count(const cpg_ctx *ctx);
 /* library version string, e.g. "cpolyg_b200 0.1 sm_100a" */

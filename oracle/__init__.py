@@ -24,6 +24,11 @@ _PROTO = {
     "orc_get_threads": (I, []),
     "orc_mesh_create": (P, [I, PI, PD, D, D, I, PI, PI, PD]),
     "orc_mesh_destroy": (None, [P]),
+    "orc_seeds_uniform": (None, [C.c_uint64, I, D, D, PD]),
+    "orc_mesh_voronoi": (P, [PD, I, D, D, I, PI]),
+    "orc_mesh_polys": (None, [P, PI, PD]),
+    "orc_mesh_nnzb": (I, [P]),
+    "orc_mesh_pattern": (None, [P, PI, PI]),
     "orc_mesh_nedges": (I, [P]),
     "orc_mesh_export": (None, [P, PI, PI, PD, PD, PD]),
     "orc_eq_create": (P, [P, I, I, D, D, D, I, PD, PD]),
@@ -95,8 +100,45 @@ def get_threads() -> int:
     return load().orc_get_threads()
 
 
+def uniform_seeds(seed: int, n: int, width: float = 1.0, height: float = 1.0) -> np.ndarray:
+    """std::mt19937_64(seed): x = (g()>>11)*2^-53*width, then y."""
+    xy = np.empty((n, 2))
+    load().orc_seeds_uniform(C.c_uint64(seed), n, width, height, pd(xy))
+    return xy
+
+
 class Mesh:
     """Oracle mesh built from cell-frame polygons + sub-triangles."""
+
+    @classmethod
+    def voronoi(cls, seeds, width: float, height: float, periodic: bool = False, side_codes=None) -> "Mesh":
+        """Brute-force (O(n^2)) Voronoi mesh of the seeds, built by the oracle
+        alone; sub-triangles are the fans from the vertex centroids."""
+        L = load()
+        xy = f64(seeds)
+        codes = None if side_codes is None else i32(side_codes)
+        self = cls.__new__(cls)
+        self.a = None
+        self._keep = (xy, codes)
+        self.n = len(xy)
+        self.h = L.orc_mesh_voronoi(pd(xy), self.n, width, height, int(periodic),
+                                    None if codes is None else pi(codes))
+        return self
+
+    def polygons(self):
+        """(cell_ptr, poly_xy) in cell frames, after vertex deduplication"""
+        L = load()
+        E = L.orc_mesh_nedges(self.h)
+        cp, xy = np.zeros(self.n + 1, np.int32), np.zeros((E, 2))
+        L.orc_mesh_polys(self.h, pi(cp), pd(xy))
+        return cp, xy
+
+    def pattern(self):
+        """Jacobian block pattern (rowptr, colidx) of the oracle's connectivity"""
+        L = load()
+        rp, cl = np.zeros(self.n + 1, np.int32), np.zeros(L.orc_mesh_nnzb(self.h), np.int32)
+        L.orc_mesh_pattern(self.h, pi(rp), pi(cl))
+        return rp, cl
 
     def __init__(self, arrays: dict, side_codes=None):
         L = load()

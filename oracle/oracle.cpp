@@ -13,7 +13,7 @@
 //   arma::inv / LAPACK dgetrf/getrs -> partial-pivot LU (dgetf2 algorithm)
 //   arma::solve (overdetermined)   -> Householder QR least squares
 //   dgemv / dnrm2 / dtpsv          -> plain loops
-// Reference defects handled explicitly (see DESIGN.md of the repository):
+// Reference defects handled explicitly:
 //   D1 periodic trace degree: periodic faces are ordinary neighbours with a
 //      coordinate shift, evaluated with the full basis;
 //   D2 MassMatrix::solve offset: uses i*bl;
@@ -30,6 +30,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <random>
 #include <string>
 #include <unordered_map>
 #include <vector>
@@ -382,6 +383,89 @@ static bool build_mesh(Mesh &m, int n, const int *cell_ptr, const double *xy, do
             m.tri[i].push_back(T);
         }
     return true;
+}
+
+// Seeds of the synthetic meshes: std::mt19937_64(seed), x = (g()>>11) 2^-53
+// scaled to the domain, then y (the same generator the library's host code
+// uses, so both read identical points).
+static void seeds_uniform(uint64_t seed, int n, double W, double H, double *xy) {
+    std::mt19937_64 g(seed);
+    for (int i = 0; i < n; i++) {
+        const double x = (double)(g() >> 11) * 0x1.0p-53, y = (double)(g() >> 11) * 0x1.0p-53;
+        xy[2 * i] = x * W;
+        xy[2 * i + 1] = y * H;
+    }
+}
+
+// Voronoi cells by brute force, independent of the library's bucket-grid
+// mesher: cell i is the domain box (periodic: the box of side 2W x 2H around
+// the seed) cut by the bisector half-plane of every other seed and, when
+// periodic, of its 8 lattice images, nearest first.  O(n^2); used for the
+// CPU-baseline sample meshes and as a check of the library's cells.  The
+// polygon is counter-clockwise in the frame of seed i; its volume quadrature
+// runs on the fan of triangles from the vertex centroid (the reference uses
+// Triangle's "zQq" sub-triangles, Triangulation.cpp:11-101; both are exact
+// for polynomial integrands).
+static void voronoi_polys(const double *xy, int n, double W, double H, bool periodic, vector<int> &cptr,
+                          vector<double> &pxy, vector<int> &tptr, vector<double> &txy) {
+    cptr.assign(1, 0);
+    pxy.clear();
+    tptr.assign(1, 0);
+    txy.clear();
+    vector<std::array<double, 3>> cand;
+    vector<std::array<double, 2>> P, Q;
+    for (int i = 0; i < n; i++) {
+        const double sx = xy[2 * i], sy = xy[2 * i + 1];
+        cand.clear();
+        const int img = periodic ? 1 : 0;
+        for (int j = 0; j < n; j++)
+            for (int a = -img; a <= img; a++)
+                for (int b = -img; b <= img; b++) {
+                    if (j == i && a == 0 && b == 0) continue;
+                    const double qx = xy[2 * j] + a * W, qy = xy[2 * j + 1] + b * H;
+                    cand.push_back({(qx - sx) * (qx - sx) + (qy - sy) * (qy - sy), qx, qy});
+                }
+        std::sort(cand.begin(), cand.end(), [](const std::array<double, 3> &u, const std::array<double, 3> &v) {
+            return u[0] < v[0];
+        });
+        if (periodic) P = {{sx - W, sy - H}, {sx + W, sy - H}, {sx + W, sy + H}, {sx - W, sy + H}};
+        else P = {{0, 0}, {W, 0}, {W, H}, {0, H}};
+        for (const auto &c : cand) {
+            // a candidate farther than twice the cell's radius cannot cut it
+            double R2 = 0;
+            for (const auto &p : P) R2 = std::max(R2, (p[0] - sx) * (p[0] - sx) + (p[1] - sy) * (p[1] - sy));
+            if (c[0] > 4 * R2) break;
+            const double dx = c[1] - sx, dy = c[2] - sy, mx = 0.5 * (c[1] + sx), my = 0.5 * (c[2] + sy);
+            Q.clear();
+            const size_t m = P.size();
+            for (size_t k = 0; k < m; k++) {
+                const auto &A = P[k], &B = P[(k + 1) % m];
+                const double fa = (A[0] - mx) * dx + (A[1] - my) * dy, fb = (B[0] - mx) * dx + (B[1] - my) * dy;
+                if (fa <= 0) Q.push_back(A);
+                if ((fa < 0 && fb > 0) || (fa > 0 && fb < 0)) {
+                    const double t = fa / (fa - fb);
+                    Q.push_back({A[0] + t * (B[0] - A[0]), A[1] + t * (B[1] - A[1])});
+                }
+            }
+            P.swap(Q);
+        }
+        double cx = 0, cy = 0;
+        for (const auto &p : P) {
+            pxy.push_back(p[0]);
+            pxy.push_back(p[1]);
+            cx += p[0];
+            cy += p[1];
+        }
+        cx /= (double)P.size();
+        cy /= (double)P.size();
+        for (size_t k = 0; k < P.size(); k++) {
+            const auto &A = P[k], &B = P[(k + 1) % P.size()];
+            const double T[6] = {cx, cy, A[0], A[1], B[0], B[1]};
+            txy.insert(txy.end(), T, T + 6);
+        }
+        cptr.push_back((int)(pxy.size() / 2));
+        tptr.push_back((int)(txy.size() / 6));
+    }
 }
 
 // polygonIntegral (Quadrature.cpp:13-57), integrand f(x, y, out[nout])
@@ -1392,7 +1476,7 @@ static void jacobi(const Op &A, const double *b, double *x, double &tol, int &ma
 // ------------------------------------------------------------------------
 enum {
     ST_FE = 0, ST_RK2 = 1, ST_RK4 = 2, ST_BE = 3, ST_DIRK3 = 4, ST_DIRK5 = 5,
-    ST_IRK2 = 6, ST_IRK3 = 7, ST_IRK2_INV = 8, ST_IRK3_INV = 9
+    ST_IRK2 = 6, ST_IRK3 = 7, ST_IRK2_INV = 8, ST_IRK3_INV = 9, ST_SDIRK3 = 10
 };
 enum { PC_NONE = 0, PC_BJACOBI = 1, PC_ILU0 = 2, PC_BJACOBI_CELL = 3 };
 
@@ -1427,6 +1511,20 @@ static void rk_stage(Stepper &S, const double *u, double t, double dt, double *k
     assemble(*S.eq, u, t, b.data());
     mass_solve(*S.M, b.data(), k);
     for (size_t q = 0; q < N; q++) k[q] = dt * k[q];
+}
+
+// Alexander's L-stable 3-stage SDIRK of order 3 (R. Alexander, SIAM J. Numer.
+// Anal. 14 (1977) 1006-1021): gamma is the root in (1/6, 1/2) of
+// g^3 - 3g^2 + 3g/2 - 1/6 = 0, the last row of A is b (stiffly accurate).
+// The reference's getDIRK(3) uses this gamma with Crouzeix's tableau
+// instead, which is of order 2 and not A-stable (|R(-inf)| = 1.78).
+static void getSDIRK3(vector<double> &A, vector<double> &b, vector<double> &c) {
+    const double g = 0.435866521508459;
+    const double t2 = (1 + g) / 2.0;
+    const double b1 = -(6 * g * g - 16 * g + 1) / 4.0, b2 = (6 * g * g - 20 * g + 5) / 4.0;
+    A = {g, 0, 0, t2 - g, g, 0, b1, b2, g};
+    b = {b1, b2, g};
+    c = {g, t2, 1.0};
 }
 
 static void getDIRK(int s, vector<double> &A, vector<double> &b, vector<double> &c) {
@@ -1513,6 +1611,9 @@ static void dirk_advance(Stepper &S, double *u, double dt, double t) {
         A = {1.0};
         b = {1.0};
         c = {1.0};
+    } else if (S.kind == ST_SDIRK3) {
+        s = 3;
+        getSDIRK3(A, b, c);
     } else {
         s = S.kind == ST_DIRK3 ? 3 : 5;
         getDIRK(s, A, b, c);
@@ -1794,7 +1895,7 @@ static void advance(Stepper &S, double *u, double dt, double t) {
         rk_stage(S, tmp.data(), t + dt, dt, k4.data());
         for (size_t q = 0; q < N; q++)
             u[q] = u[q] + (((k1[q] + 2 * k2[q]) + 2 * k3[q]) + k4[q]) * (1.0 / 6.0);
-    } else if (S.kind == ST_BE || S.kind == ST_DIRK3 || S.kind == ST_DIRK5) {
+    } else if (S.kind == ST_BE || S.kind == ST_DIRK3 || S.kind == ST_DIRK5 || S.kind == ST_SDIRK3) {
         dirk_advance(S, u, dt, t);
     } else if (S.kind == ST_IRK2 || S.kind == ST_IRK3) {
         irk_advance(S, u, dt, t);
@@ -1871,6 +1972,48 @@ orc_mesh *orc_mesh_create(int n, const int *cell_ptr, const double *poly_xy, dou
     orc_mesh *h = new orc_mesh();
     build_mesh(h->m, n, cell_ptr, poly_xy, W, H, periodic, codes, tri_ptr, tri_xy);
     return h;
+}
+// seeds (std::mt19937_64 spec) and a brute-force Voronoi mesh of them
+void orc_seeds_uniform(uint64_t seed, int n, double W, double H, double *xy) { seeds_uniform(seed, n, W, H, xy); }
+orc_mesh *orc_mesh_voronoi(const double *xy, int n, double W, double H, int periodic, const int *codes) {
+    vector<int> cptr, tptr;
+    vector<double> pxy, txy;
+    voronoi_polys(xy, n, W, H, periodic != 0, cptr, pxy, tptr, txy);
+    orc_mesh *h = new orc_mesh();
+    build_mesh(h->m, n, cptr.data(), pxy.data(), W, H, periodic, codes, tptr.data(), txy.data());
+    return h;
+}
+// cell-frame polygons of an oracle mesh (after vertex deduplication)
+void orc_mesh_polys(orc_mesh *h, int *cell_ptr, double *poly_xy) {
+    const Mesh &m = h->m;
+    int e = 0;
+    cell_ptr[0] = 0;
+    for (int i = 0; i < m.np; i++) {
+        for (const auto &q : m.pv[i]) {
+            poly_xy[2 * e] = q[0];
+            poly_xy[2 * e + 1] = q[1];
+            e++;
+        }
+        cell_ptr[i + 1] = e;
+    }
+}
+// Jacobian block pattern (Jacobian ctor, Jacobian.cpp:7-47) without values
+int orc_mesh_nnzb(orc_mesh *h) {
+    int nnzb = h->m.np;
+    for (const auto &q : h->m.p2p)
+        for (int k : q) nnzb += k >= 0;
+    return nnzb;
+}
+void orc_mesh_pattern(orc_mesh *h, int *rowptr, int *col) {
+    const Mesh &m = h->m;
+    int k = 0;
+    for (int i = 0; i < m.np; i++) {
+        rowptr[i] = k;
+        col[k++] = i;
+        for (int j : m.p2p[i])
+            if (j >= 0) col[k++] = j;
+    }
+    rowptr[m.np] = k;
 }
 void orc_mesh_destroy(orc_mesh *h) { delete h; }
 int orc_mesh_nedges(orc_mesh *h) {

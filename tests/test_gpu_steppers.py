@@ -179,3 +179,76 @@ def test_explicit_step_graph_replay_matches_direct_launches(ctx):
         assert sctx.launches - launches0 == ctx.launches - direct0
     torch.cuda.synchronize()
     assert torch.equal(ua, ub)
+
+
+# ---------------------------------------------------------------------------
+# The benchmark's time step on an oracle-sized mesh: the 100k-cell vortex's
+# dt = 0.05 scaled by the cell size (dt = 0.05 * sqrt(100000 / n), the same
+# dt/h), 20 steps of Alexander's L-stable SDIRK3, against the oracle's run
+# recorded in tests/golden/sdirk3_vortex_p3_1000.npz (make_golden.py).
+# ---------------------------------------------------------------------------
+def _golden_sdirk3():
+    import os
+
+    from golden.make_golden import mesh_digest
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "sdirk3_vortex_p3_1000.npz"))
+    m = cp.PolyMesh.voronoi(cp.uniform_seeds(int(g["seed"]), int(g["n"]), 10.0, 10.0), 10.0, 10.0, periodic=True)
+    assert mesh_digest(m.export()) == str(g["mesh_sha256"]), "the mesh differs from the one the fixture was made on"
+    return g, m
+
+
+def _run_sdirk3(ctx, g, m, **kw):
+    eq = cp.Euler(ctx, m, int(g["degree"]), dirichlet=(cp.INIT_VORTEX, VORTEX[1]), exact_jacobian=True)
+    u = eq.interp(cp.INIT_VORTEX, VORTEX[1])
+    assert l2rel(to_np(u), g["u0"]) < 1e-13
+    st = cp.SDIRK3(eq, pc=cp.PC_ILU0, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000, **kw)
+    dt, t, newton = float(g["dt"]), 0.0, []
+    for _ in range(int(g["steps"])):
+        st.advance(u, dt, t)
+        assert st.stats.converged == 1
+        newton.append(st.stats.newton_iterations)
+        t += dt
+    return to_np(u), newton
+
+
+def test_sdirk3_vortex_20_steps_at_benchmark_cfl(ctx):
+    """FP64: <= 1e-11 against the oracle after 20 steps, with the oracle's
+    Newton iteration count at every step."""
+    g, m = _golden_sdirk3()
+    u, newton = _run_sdirk3(ctx, g, m)
+    assert l2rel(u, g["u"]) < 1e-11
+    assert newton == [int(x) for x in g["newton"]]
+
+
+def test_sdirk3_vortex_mixed_precision_20_steps(ctx):
+    """Mixed precision (FP32 Jacobian and ILU(0) factors, FP64 FGMRES with
+    FP64 residuals, Newton update rule 1e-10) stays within 1e-8 of the FP64
+    oracle at the final time."""
+    g, m = _golden_sdirk3()
+    u, _ = _run_sdirk3(ctx, g, m, precision=cp.F32, flexible=True, newton_rtol=1e-10)
+    assert l2rel(u, g["u"]) < 1e-8
+
+
+def test_nonphysical_state_is_reported_by_name(ctx):
+    """A negative pressure planted in one cell of the host-built state makes
+    the first residual return CPG_ERR_NONPHYSICAL naming that cell (instead of
+    a NaN hidden by the flux's max and a singular pivot later), and the
+    Rusanov flux carries the NaN sound speed into the residual."""
+    import torch
+    ge, oe, _ = equations(ctx, "euler", 2, n=200, periodic=True, width=10.0)
+    u0 = oe.interp(*VORTEX).reshape(ge.np, ge.nc, ge.nb)
+    bad = 37
+    u0[bad, 3, 0] = -1.0  # energy below the kinetic energy: p < 0 in the whole cell
+    u = to_dev(u0).reshape(ge.np, ge.nc, ge.nb)
+    b = torch.empty_like(u)
+    with pytest.raises(cp.CpgError) as e:
+        ctx.check(ctx._lib.cpg_assemble(ctx.h, ge.h, cp.C.c_void_p(u.data_ptr()), 0.0, cp.C.c_void_p(b.data_ptr())))
+    assert e.value.status == 10 and f"cell {bad}" in str(e.value)
+    assert not torch.isfinite(b[bad]).all()
+    # the context stays usable and the word was cleared: a good state passes
+    ug = to_dev(oe.interp(*VORTEX)).reshape(ge.np, ge.nc, ge.nb)
+    ge.assemble(ug)
+    step = cp.SDIRK3(ge, pc=cp.PC_ILU0, gmres_m=30, gmres_tol=1e-10)
+    with pytest.raises(cp.CpgError) as e:
+        step.advance(u, 0.05, 0.0)
+    assert e.value.status == 10 and f"cell {bad}" in str(e.value) and "Newton iteration 0" in str(e.value)

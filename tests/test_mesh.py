@@ -106,3 +106,54 @@ def test_quad_mesh_from_polygons():
     # coarse periodic meshes whose cells meet twice are rejected
     with pytest.raises(cp.CpgError):
         cp.PolyMesh.voronoi(cp.uniform_seeds(3, 3), 1, 1, periodic=True)
+
+
+def _rotate_to_match(P, Q):
+    """rotation of the cyclic vertex list Q that best matches P (max abs diff)"""
+    best = None
+    for r in range(len(Q)):
+        d = np.abs(np.roll(Q, -r, axis=0) - P).max()
+        best = d if best is None else min(best, d)
+    return best
+
+
+@pytest.mark.parametrize("n,periodic,width,seed", [(2000, True, 10.0, 2), (1500, False, 1.0, 1)])
+def test_voronoi_cells_match_brute_force_oracle(n, periodic, width, seed):
+    """The library's bucket-grid mesher against the oracle's brute-force
+    half-plane clipping of the same seeds: same polygons vertex for vertex
+    (up to the start vertex, within 1e-9 of the domain size) and the same
+    neighbour set of every cell, periodic and not."""
+    seeds = cp.uniform_seeds(seed, n, width, width)
+    assert np.array_equal(seeds, oracle.uniform_seeds(seed, n, width, width))
+    m = cp.PolyMesh.voronoi(seeds, width, width, periodic=periodic)
+    a = m.export()
+    om = oracle.Mesh.voronoi(seeds, width, width, periodic=periodic)
+    ocp, oxy = om.polygons()
+    onbr = om.export()["edge_nbr"]
+    assert np.array_equal(np.diff(ocp), np.diff(a["cell_ptr"]))
+    for i in range(n):
+        P = a["poly_xy"][a["cell_ptr"][i]:a["cell_ptr"][i + 1]]
+        Q = oxy[ocp[i]:ocp[i + 1]]
+        assert _rotate_to_match(P, Q) < 1e-9 * width
+        assert set(a["edge_nbr"][a["cell_ptr"][i]:a["cell_ptr"][i + 1]]) == set(onbr[ocp[i]:ocp[i + 1]])
+
+
+def test_benchmark_mesh_pattern_and_levels_match_oracle():
+    """The 100k-cell periodic benchmark mesh (seed 2, [0,10]^2): edge
+    neighbours, periodic shifts, bounding boxes, the Jacobian block pattern
+    (Jacobian ctor, src/Jacobian.cpp:7-47) and the ILU(0) level schedule
+    (the dependency order of src/Preconditioners.cpp:49-158), derived by the
+    oracle from the cell polygons alone, byte for byte."""
+    seeds = cp.uniform_seeds(2, 100000, 10.0, 10.0)
+    m = cp.PolyMesh.voronoi(seeds, 10.0, 10.0, periodic=True)
+    a = m.export()
+    om = oracle.Mesh(a)
+    o = om.export()
+    for k in ("cell_ptr", "edge_nbr", "edge_shift", "bb"):
+        assert np.array_equal(o[k], a[k]), k
+    rp, cl = m.pattern()
+    orp, ocl = om.pattern()
+    assert np.array_equal(rp, orp) and np.array_equal(cl, ocl)
+    assert len(cl) == 100000 + len(a["edge_nbr"])
+    for x, y in zip(cp.pattern_levels(rp, cl), oracle.levels(rp, cl)):
+        assert np.array_equal(x, y)

@@ -295,6 +295,84 @@ def test_dirk3_tableau_is_second_order():
     assert 3 < r < 5
 
 
+def _tableau(kind):
+    """(A, b) of the implicit tableaux, written out independently of the
+    oracle and the library (src/TimeIntegration.cpp:68-186)."""
+    r6 = np.sqrt(6.0)
+    if kind == "dirk3_reference":
+        a = 0.435866521508459
+        A = [[(1 + a) / 2, 0, 0], [-a / 2, (1 + a) / 2, 0], [1 + a, -(1 + 2 * a), (1 + a) / 2]]
+        b = [1 / 6 / a ** 2, 1 - 1 / 3 / a ** 2, 1 / 6 / a ** 2]
+    elif kind == "sdirk3":
+        g = 0.435866521508459
+        b1, b2 = -(6 * g * g - 16 * g + 1) / 4, (6 * g * g - 20 * g + 5) / 4
+        A = [[g, 0, 0], [(1 - g) / 2, g, 0], [b1, b2, g]]
+        b = [b1, b2, g]
+    elif kind == "backward_euler":
+        A, b = [[1.0]], [1.0]
+    elif kind == "dirk5":
+        g = (6 - r6) / 10
+        A = [[g, 0, 0, 0, 0], [(-6 + 5 * r6) / 14, g, 0, 0, 0],
+             [(888 + 607 * r6) / 2850, (126 - 161 * r6) / 1425, g, 0, 0],
+             [(3153 - 3082 * r6) / 14250, (3213 + 1148 * r6) / 28500, (-267 + 88 * r6) / 500, g, 0],
+             [(-32583 + 14638 * r6) / 71250, (-17199 + 364 * r6) / 142500, (1329 - 544 * r6) / 2500,
+              (-96 + 131 * r6) / 625, g]]
+        b = [0, 0, 1 / 9, (16 - r6) / 36, (16 + r6) / 36]
+    elif kind == "radau2":
+        A, b = [[5 / 12, -1 / 12], [3 / 4, 1 / 4]], [3 / 4, 1 / 4]
+    else:  # radau3
+        A = [[(88 - 7 * r6) / 360, (296 - 169 * r6) / 1800, (-2 + 3 * r6) / 225],
+             [(296 + 169 * r6) / 1800, (88 + 7 * r6) / 360, (-2 - 3 * r6) / 225],
+             [(16 - r6) / 36, (16 + r6) / 36, 1 / 9]]
+        b = [(16 - r6) / 36, (16 + r6) / 36, 1 / 9]
+    return np.array(A, dtype=np.float64), np.array(b, dtype=np.float64)
+
+
+def stability(A, b, z):
+    """R(z) = 1 + z b^T (I - zA)^{-1} 1"""
+    s = len(b)
+    return 1 + z * b @ np.linalg.solve(np.eye(s) - z * A, np.ones(s))
+
+
+@pytest.mark.parametrize("kind", ["sdirk3", "backward_euler", "dirk5", "radau2", "radau3"])
+def test_implicit_tableaux_are_a_stable(kind):
+    """|R(z)| <= 1 on the closed left half-plane for every implicit tableau a
+    benchmark runs.  R is rational with poles at the reciprocals of A's
+    eigenvalues; with all of them in the right half-plane, the maximum
+    principle reduces the check to the imaginary axis (sampled densely, plus
+    z -> infinity along the negative real axis)."""
+    A, b = _tableau(kind)
+    assert (np.linalg.eigvals(A).real > 0).all()
+    ys = np.concatenate([np.linspace(-50, 50, 20001), np.geomspace(50, 1e8, 2000)])
+    mx = max(abs(stability(A, b, 1j * y)) for y in np.concatenate([ys, -ys]))
+    assert mx <= 1 + 1e-12
+    assert abs(stability(A, b, -1e12)) <= 1.0
+
+
+def test_reference_dirk3_tableau_is_not_a_stable():
+    """The reference's getDIRK(3) amplifies stiff modes: |R(-inf)| = 1.78 and
+    |R(-10)| = 1.20, so at the 100k-cell vortex's time step (CFL ~ 50 for the
+    p=3 modes) the scheme is unstable; benchmarks run SDIRK3 instead."""
+    A, b = _tableau("dirk3_reference")
+    assert abs(stability(A, b, -1e12)) > 1.7
+    assert abs(stability(A, b, -10.0)) > 1.15
+
+
+def test_sdirk3_is_third_order_and_l_stable():
+    """Alexander's SDIRK3: order-3 conditions, stiffly accurate, R(-inf) = 0;
+    the oracle's temporal order on advection is 3 (error ratio ~8 per
+    halving of dt)."""
+    A, b = _tableau("sdirk3")
+    c = A.sum(1)
+    assert abs(b.sum() - 1) < 1e-14 and abs(b @ c - 1 / 2) < 1e-14
+    assert abs(b @ c ** 2 - 1 / 3) < 1e-14 and abs(b @ A @ c - 1 / 6) < 1e-14
+    assert np.array_equal(A[-1], b)
+    assert abs(stability(A, b, -1e12)) < 1e-6
+    u = temporal_error(10, [0.004, 0.002, 0.001], 0.016)
+    r = np.linalg.norm(u[0] - u[1]) / np.linalg.norm(u[1] - u[2])
+    assert 6.5 < r < 9.5
+
+
 def test_radau_iia_third_order():
     u = temporal_error(6, [0.004, 0.002, 0.001], 0.016)
     r = np.linalg.norm(u[0] - u[1]) / np.linalg.norm(u[1] - u[2])
