@@ -62,7 +62,7 @@ def sdirk3_vortex(n: int = 1000, degree: int = 3, steps: int = 20) -> dict:
         gmres.append(int(st.stats[1]))
         print(f"  step {k + 1}: newton {newton[-1]} gmres {gmres[-1]} ({time.time() - t0:.1f} s)", flush=True)
         assert st.stats[3] == 1, "oracle Newton did not converge"
-    return dict(n=n, degree=degree, seed=2, dt=dt, steps=steps, mesh_sha256=mesh_digest(arrays), u0=u0, u=u,
+    return dict(n=n, degree=degree, seed=2, dt=dt, steps=steps, mesh_sha256=mesh_digest(arrays), u=u,
                 newton=np.array(newton), gmres=np.array(gmres))
 
 

@@ -200,7 +200,6 @@ def _golden_sdirk3():
 def _run_sdirk3(ctx, g, m, **kw):
     eq = cp.Euler(ctx, m, int(g["degree"]), dirichlet=(cp.INIT_VORTEX, VORTEX[1]), exact_jacobian=True)
     u = eq.interp(cp.INIT_VORTEX, VORTEX[1])
-    assert l2rel(to_np(u), g["u0"]) < 1e-13
     st = cp.SDIRK3(eq, pc=cp.PC_ILU0, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000, **kw)
     dt, t, newton = float(g["dt"]), 0.0, []
     for _ in range(int(g["steps"])):
