@@ -269,6 +269,15 @@ class Equation:
         self.ctx.check(self._lib.cpg_l2norm(self.ctx.h, self.h, C.c_void_p(_ptr(u)), _pd(out)))
         return out[: self.nc].copy()
 
+    def L2Error(self, u, kind: int, params, t: float = 0.0) -> np.ndarray:
+        """MeshFn::L2Error (src/MeshFn.cpp:283-296) against the analytic field
+        (kind, params) at time t, per component."""
+        p = np.zeros(8)
+        p[: len(params)] = params
+        out = np.zeros(4)
+        self.ctx.check(self._lib.cpg_l2error(self.ctx.h, self.h, C.c_void_p(_ptr(u)), kind, _pd(p), t, _pd(out)))
+        return out[: self.nc]
+
     def __del__(self):
         try:
             if self.h:

@@ -94,6 +94,7 @@ PROTOTYPES = {
     "cpg_mass_solve": (I, [P, P, P, P]),
     "cpg_l2norm": (I, [P, P, P, PD]),
     "cpg_l2norm_noalloc": (I, [P, P, P, PD]),
+    "cpg_l2error": (I, [P, P, P, I, PD, D, PD]),
     "cpg_interp": (I, [P, P, I, PD, D, P]),
     "cpg_mass_export": (I, [P, P, PD]),
     "cpg_bsr_create": (I, [P, P, I, PP]),

@@ -372,6 +372,44 @@ __global__ void k_l2_partial(int n, int nc, const double *__restrict__ M, const 
     }
     if (threadIdx.x < 4) part[blockIdx.x * 4 + threadIdx.x] = sh[threadIdx.x][0];
 }
+// per-CTA partial sums of sum_q w_q (u_h(x_q) - exact(x_q))^2 over the cells'
+// volume quadrature points (MeshFn::L2Error); fixed grid, deterministic
+template <int P, int NC>
+__global__ void k_l2_error_partial(Geo g, int kind, BCParams prm, double t, const double *__restrict__ u,
+                                   double *__restrict__ part) {
+    constexpr int NB = nbasis<P>(), BL = NB * NC;
+    __shared__ double sh[4][256];
+    double acc[4] = {0, 0, 0, 0};
+    for (int cell = blockIdx.x * blockDim.x + threadIdx.x; cell < g.n; cell += gridDim.x * blockDim.x) {
+        const double *uc = u + (size_t)cell * BL;
+        double cs[NC];
+#pragma unroll
+        for (int c = 0; c < NC; c++) cs[c] = 0.0;
+        for (int q = g.vq_ptr[cell]; q < g.vq_ptr[cell + 1]; q++) {
+            double psi[NB], ex[NC];
+            basis<P>(g.vxi[q], g.veta[q], psi);
+            field_eval<NC>(kind, prm.dparams, g.vx[q], g.vy[q], t, ex);
+#pragma unroll
+            for (int c = 0; c < NC; c++) {
+                double v = 0.0;
+#pragma unroll
+                for (int k = 0; k < NB; k++) v += uc[c * NB + k] * psi[k];
+                const double d = v - ex[c];
+                cs[c] += g.vw[q] * (d * d);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[c] += cs[c];
+    }
+    for (int c = 0; c < 4; c++) sh[c][threadIdx.x] = acc[c];
+    __syncthreads();
+    for (int off = blockDim.x / 2; off > 0; off >>= 1) {
+        if ((int)threadIdx.x < off)
+            for (int c = 0; c < 4; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + off];
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) part[blockIdx.x * 4 + threadIdx.x] = sh[threadIdx.x][0];
+}
 __global__ void k_l2_final(int nparts, const double *__restrict__ part, double *__restrict__ out) {
     const int c = threadIdx.x;
     if (c >= 4) return;
@@ -854,6 +892,38 @@ cpg_status cpg_l2norm(cpg_ctx *ctx, const cpg_equation *eq, const double *u, dou
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     for (int c = 0; c < eq->nc; c++) {
         if (!std::isfinite(hp[c])) return fail(ctx, CPG_ERR_NONFINITE, "non-finite L2 norm");
+        out_host[c] = std::sqrt(std::max(0.0, hp[c]));
+    }
+    return CPG_OK;
+}
+
+cpg_status cpg_l2error(cpg_ctx *ctx, const cpg_equation *eq, const double *u, int kind, const double *params,
+                       double t, double *out_host) {
+    if (!ctx || !eq || !u || !out_host || kind < 0 || kind > 3) return CPG_ERR_INVALID_ARG;
+    BCParams prm{};
+    for (int q = 0; q < 8; q++) prm.dparams[q] = params ? params[q] : 0.0;
+    double *part, *hp;
+    CPG_TRY(scratch(ctx, RED_CTAS * 4 + 4, &part));
+    CPG_TRY(pinned(ctx, 4, &hp));
+    const Geo g = eq->geo();
+    auto launch = [&](auto pc) {
+        constexpr int P = decltype(pc)::value;
+        if (eq->nc == 4) k_l2_error_partial<P, 4><<<RED_CTAS, 256, 0, ctx->stream>>>(g, kind, prm, t, u, part);
+        else k_l2_error_partial<P, 1><<<RED_CTAS, 256, 0, ctx->stream>>>(g, kind, prm, t, u, part);
+    };
+    switch (eq->degree) {
+        case 1: launch(std::integral_constant<int, 1>{}); break;
+        case 2: launch(std::integral_constant<int, 2>{}); break;
+        case 3: launch(std::integral_constant<int, 3>{}); break;
+        default: return fail(ctx, CPG_ERR_UNSUPPORTED, "degree must be 1..3");
+    }
+    CPG_TRY(launched(ctx, "l2 error kernel"));
+    k_l2_final<<<1, 32, 0, ctx->stream>>>(RED_CTAS, part, part + RED_CTAS * 4);
+    CPG_TRY(launched(ctx, "l2 final kernel"));
+    CPG_CUDA(ctx, cudaMemcpyAsync(hp, part + RED_CTAS * 4, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int c = 0; c < eq->nc; c++) {
+        if (!std::isfinite(hp[c])) return fail(ctx, CPG_ERR_NONFINITE, "non-finite L2 error");
         out_host[c] = std::sqrt(std::max(0.0, hp[c]));
     }
     return CPG_OK;

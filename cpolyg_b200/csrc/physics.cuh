@@ -14,7 +14,10 @@ __host__ __device__ inline void field_eval(int kind, const double *P, double x, 
     if (kind == CPG_INIT_CONSTANT) {
         for (int c = 0; c < NC; c++) out[c] = P[c];
     } else if (kind == CPG_INIT_GAUSSIAN) {
-        const double dx = x - P[1], dy = y - P[2];
+        // centre (x0, y0) + (bx, by) t, nearest periodic image when Lx, Ly > 0
+        double dx = x - (P[1] + P[3] * t), dy = y - (P[2] + P[4] * t);
+        if (P[5] > 0) dx -= P[5] * round(dx / P[5]);
+        if (P[6] > 0) dy -= P[6] * round(dy / P[6]);
         out[0] = exp(-P[0] * (dx * dx + dy * dy));
         for (int c = 1; c < NC; c++) out[c] = 0.0;
     } else if (kind == CPG_INIT_VORTEX) {

@@ -76,8 +76,11 @@ typedef enum {
  * Dirichlet states                                                           */
 typedef enum {
     CPG_INIT_CONSTANT = 0,     /* params[0..nc-1] = state                     */
-    CPG_INIT_GAUSSIAN = 1,     /* scalar: exp(-a((x-x0)^2+(y-y0)^2)),
-                                  params = {a, x0, y0}                         */
+    CPG_INIT_GAUSSIAN = 1,     /* scalar: exp(-a((x-x0-bx t)^2+(y-y0-by t)^2)),
+                                  params = {a, x0, y0, bx, by, Lx, Ly}: the
+                                  centre moves with (bx, by); Lx, Ly > 0 take
+                                  the nearest periodic image (the exact
+                                  solution of constant advection)             */
     CPG_INIT_VORTEX = 2,       /* isentropic vortex, params =
                                   {beta, x0, y0, uinf, vinf, gamma, Lx, Ly}   */
     CPG_INIT_DENSITY_BUMP = 3  /* Euler: rho = 1 + A exp(-r^2/w^2), uniform
@@ -266,6 +269,12 @@ cpg_status cpg_l2norm(cpg_ctx *ctx, const cpg_equation *eq,
  * serialized by the caller.                                                 */
 cpg_status cpg_l2norm_noalloc(cpg_ctx *ctx, const cpg_equation *eq,
                               const double *u_dev, double *out_host);
+/* MeshFn::L2Error (src/MeshFn.cpp:283-296): per-component
+ * sqrt(sum_K int_K (u_h - exact)^2) with the degree-2p rule on the cells'
+ * quadrature points, exact = the analytic field (init_kind, params) at
+ * time t; out_host[nc].                                                     */
+cpg_status cpg_l2error(cpg_ctx *ctx, const cpg_equation *eq, const double *u_dev, int init_kind,
+                       const double *params, double t, double *out_host);
 /* MeshFn::interp (src/MeshFn.cpp:56-145): least-squares projection on the
  * (p+1)^2 Gauss grid of each bounding box of an analytic field.             */
 cpg_status cpg_interp(cpg_ctx *ctx, const cpg_equation *eq, int init_kind,

@@ -41,6 +41,7 @@ _PROTO = {
     "orc_mass_solve": (None, [P, PD, PD]),
     "orc_mass_matvec": (None, [P, PD, PD]),
     "orc_l2norm": (None, [P, PD, PD]),
+    "orc_l2error": (None, [P, PD, I, PD, D, PD]),
     "orc_interp": (None, [P, I, PD, D, PD]),
     "orc_bsr_matvec": (None, [I, I, PI, PI, PD, PD, PD]),
     "orc_ilu0": (I, [I, I, PI, PI, PD, PD, PI, PI, PD, PI, PI, PD]),
@@ -233,6 +234,14 @@ class Equation:
         u = f64(u).ravel()
         out = np.zeros(4)
         load().orc_l2norm(self.h, pd(u), pd(out))
+        return out[: self.nc]
+
+    def l2error(self, u, kind, params, t=0.0):
+        u = f64(u).ravel()
+        p = np.zeros(8)
+        p[: len(params)] = params
+        out = np.zeros(4)
+        load().orc_l2error(self.h, pd(u), kind, pd(p), t, pd(out))
         return out[: self.nc]
 
     def interp(self, kind, params, t=0.0):

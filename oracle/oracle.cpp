@@ -519,7 +519,10 @@ static void field_eval(int kind, const double *P, int nc, double x, double y, do
     if (kind == INIT_CONSTANT) {
         for (int c = 0; c < nc; c++) out[c] = P[c];
     } else if (kind == INIT_GAUSSIAN) {
-        const double dx = x - P[1], dy = y - P[2];
+        // centre (x0, y0) + (bx, by) t, nearest periodic image when Lx, Ly > 0
+        double dx = x - (P[1] + P[3] * t), dy = y - (P[2] + P[4] * t);
+        if (P[5] > 0) dx -= P[5] * std::round(dx / P[5]);
+        if (P[6] > 0) dy -= P[6] * std::round(dy / P[6]);
         out[0] = std::exp(-P[0] * (dx * dx + dy * dy));
         for (int c = 1; c < nc; c++) out[c] = 0;
     } else if (kind == INIT_VORTEX) {
@@ -1097,6 +1100,26 @@ static void l2norm(const Equation &eq, const double *u, double *out) {
         for (int c = 0; c < nc; c++) l2[c] += integ[c];
     }
     for (int c = 0; c < nc; c++) out[c] = std::sqrt(l2[c]);
+}
+
+// MeshFn::L2Error (MeshFn.cpp:283-296 with L2Difference :249-261): per
+// component sqrt(sum_K int_K (u_h - exact)^2) with the rule of degree 2p
+static void l2error(const Equation &eq, const double *u, int kind, const double *P, double t, double *out) {
+    const Mesh &msh = *eq.msh;
+    const int nc = eq.nc, bl = eq.bl, nb = eq.nb, m = eq.deg + 1;
+    vector<double> err(nc, 0.0);
+    for (int i = 0; i < msh.np; i++) {
+        double integ[4];
+        polygonIntegral(msh, i, eq.deg * 2, nc, [&](double x, double y, double *o) {
+            double xx, yy, ex[4];
+            msh.getLocalCoordinates(i, x, y, xx, yy);
+            field_eval(kind, P, nc, x, y, t, ex);
+            for (int c = 0; c < nc; c++)
+                o[c] = std::pow(Leg2D(xx, yy, m, u + (size_t)bl * i + c * nb) - ex[c], 2);
+        }, integ);
+        for (int c = 0; c < nc; c++) err[c] += integ[c];
+    }
+    for (int c = 0; c < nc; c++) out[c] = std::sqrt(err[c]);
 }
 
 // Gauss-Legendre nodes of order m (gsl glfixed restated), ascending
@@ -2084,6 +2107,9 @@ void orc_mass_blocks(orc_eq *h, double *out) {
 void orc_mass_solve(orc_eq *h, const double *x, double *y) { mass_solve(h->M, x, y); }
 void orc_mass_matvec(orc_eq *h, const double *x, double *y) { mass_matvec(h->M, x, y); }
 void orc_l2norm(orc_eq *h, const double *u, double *out) { l2norm(h->e, u, out); }
+void orc_l2error(orc_eq *h, const double *u, int kind, const double *params, double t, double *out) {
+    l2error(h->e, u, kind, params, t, out);
+}
 void orc_interp(orc_eq *h, int kind, const double *params, double t, double *u) {
     interp(h->e, kind, params, t, u);
 }

@@ -93,6 +93,26 @@ def test_mass_norm_interp(ctx, name, deg):
     assert rel(ge.L2Norm(u_gpu), oe.l2norm(u_or)) < TOL
 
 
+@pytest.mark.parametrize("name,deg,kind,params,t", [
+    ("adv_const", 2, cp.INIT_GAUSSIAN, [30.0, 0.4, 0.6, 1.0, 1.0, 1.0, 1.0], 0.35),
+    ("adv_const", 3, cp.INIT_GAUSSIAN, [30.0, 0.4, 0.6], 0.0),
+    ("euler", 3, cp.INIT_VORTEX, [5.0, 0.5, 0.5, 1, 1, 1.4, 1, 1], 0.3),
+    ("euler", 2, cp.INIT_DENSITY_BUMP, [0.1, 0.2, 0.5, 0.5, 0.3, 1.4], 0.0)])
+def test_l2_error(ctx, name, deg, kind, params, t):
+    """MeshFn::L2Error against the oracle's quadrature over the same points,
+    for a perturbed field and for the interpolant itself (<= 1e-12 relative
+    to the norm of the exact field, which bounds the rounding of the sum)."""
+    ge, oe, _ = equations(ctx, name, deg, n=300, periodic=True)
+    u_or = oe.interp(kind, params, t)
+    u_or = u_or + 0.01 * np.random.default_rng(1).standard_normal(u_or.size)
+    scale = np.linalg.norm(oe.l2error(np.zeros_like(u_or), kind, params, t))
+    eo = oe.l2error(u_or, kind, params, t)
+    eg = ge.L2Error(to_dev(u_or).reshape(ge.np, ge.nc, ge.nb), kind, params, t)
+    assert np.abs(eg - eo).max() < 1e-12 * scale
+    ui = ge.interp(kind, params, t)
+    assert np.abs(ge.L2Error(ui, kind, params, t) - oe.l2error(to_np(ui), kind, params, t)).max() < 1e-12 * scale
+
+
 BLS = [1, 3, 4, 6, 7, 10, 12, 24, 40, 48]
 
 

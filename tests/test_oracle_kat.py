@@ -377,3 +377,20 @@ def test_radau_iia_third_order():
     u = temporal_error(6, [0.004, 0.002, 0.001], 0.016)
     r = np.linalg.norm(u[0] - u[1]) / np.linalg.norm(u[1] - u[2])
     assert 6 < r < 10
+
+
+def test_l2error_of_zero_field_is_the_exact_norm():
+    """MeshFn::L2Error of the zero field is the L2 norm of the exact field:
+    for exp(-a r^2) well inside the periodic unit square that is
+    sqrt(pi / (2a)); the moving, wrapped centre gives the same value."""
+    _, a, om = mesh(1000, True, 1.0, 1)
+    eq = oracle.Equation(om, 0, 3, beta=(1.0, 1.0))
+    z = np.zeros(eq.ndof)
+    a_ = 100.0
+    want = np.sqrt(np.pi / (2 * a_))
+    e0 = eq.l2error(z, 1, [a_, 0.5, 0.5])[0]
+    e1 = eq.l2error(z, 1, [a_, 0.1, 0.2, 1.0, 1.0, 1.0, 1.0], t=0.4)[0]  # centre (0.5, 0.6)
+    assert abs(e0 - want) < 1e-3 * want and abs(e1 - want) < 1e-3 * want
+    # the interpolant of a constant state has no error
+    u = eq.interp(0, [0.7])
+    assert eq.l2error(u, 0, [0.7])[0] < 1e-13
