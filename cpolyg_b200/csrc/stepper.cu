@@ -470,9 +470,11 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
             CPG_TRY(assemble_raw(ctx, S->eq, S->cu, ts, S->rhs));
             CPG_TRY(mass_apply_axpy(ctx, S->eq, ks, 1.0, S->rhs, -dt, S->r));  // r = M k - dt rhs
             double nr;
-            CPG_TRY(newton_norm(S, S->r, &nr));
+            // a non-physical state names its cell before its NaN norm fails
+            const cpg_status ns = newton_norm(S, S->r, &nr);
             CPG_TRY(check_state(ctx, "DIRK stage " + std::to_string(stage) + ", Newton iteration " +
                                          std::to_string(iter) + ", t = " + std::to_string(ts)));
+            CPG_TRY(ns);
             st->last_newton_residual = nr;
             if (nr < S->d.newton_tol && (S->d.newton_rtol <= 0 || upd_rel < S->d.newton_rtol)) break;
             st->newton_iterations++;
@@ -545,7 +547,10 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                 CPG_TRY(assemble_raw(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
                 CPG_TRY(mass_apply_axpy(ctx, S->eq, S->tmp, 1.0, S->rhs, -dt, R + i * N));
                 double nr;
-                CPG_TRY(newton_norm(S, R + i * N, &nr));
+                const cpg_status ns = newton_norm(S, R + i * N, &nr);
+                CPG_TRY(check_state(ctx, "implicit RK stage " + std::to_string(i) + ", Newton iteration " +
+                                             std::to_string(iter) + ", t = " + std::to_string(t)));
+                CPG_TRY(ns);
                 rNorm += nr * nr;
             }
         } else {
@@ -561,12 +566,14 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                 CPG_TRY(assemble_raw(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
                 CPG_TRY(mass_apply_axpy(ctx, S->eq, K + i * N, 1.0, S->rhs, -dt, R + i * N));
                 double nr;
-                CPG_TRY(newton_norm(S, R + i * N, &nr));
+                const cpg_status ns = newton_norm(S, R + i * N, &nr);
+                CPG_TRY(check_state(ctx, "implicit RK stage " + std::to_string(i) + ", Newton iteration " +
+                                             std::to_string(iter) + ", t = " + std::to_string(t)));
+                CPG_TRY(ns);
                 rNorm += nr * nr;
             }
         }
         rNorm = std::sqrt(rNorm);
-        CPG_TRY(check_state(ctx, "implicit RK Newton iteration " + std::to_string(iter) + ", t = " + std::to_string(t)));
         st->last_newton_residual = rNorm;
         if (rNorm < S->d.newton_tol && (S->d.newton_rtol <= 0 || upd_rel < S->d.newton_rtol)) break;
         st->newton_iterations++;

@@ -84,3 +84,47 @@ def test_sync_free_sweep_waits_run_out_and_report(ctx):
     x = np.random.default_rng(0).standard_normal((len(rp) - 1) * 6)
     y = to_np(P.solve(to_dev(x)))
     assert rel(y, oracle.precond_apply(2, rp, cl, blocks, x)) < 1e-11
+
+
+def _forms(ctx, monkeypatch, A, prec, forms):
+    out = {}
+    for f in forms:
+        monkeypatch.setenv("CPG_ILU_SWEEP", f"form{f}")
+        out[f] = cp.BlockILU0(A, precision=prec)
+        assert cp.lib().cpg_precond_sweep_form(out[f].h) == f
+    monkeypatch.delenv("CPG_ILU_SWEEP")
+    return out
+
+
+@pytest.mark.parametrize("prec", [cp.F64, cp.F32])
+def test_sweep_forms_at_scale_on_the_newton_matrix(ctx, monkeypatch, prec):
+    """20,000 block rows of 40x40 (the p=3 Euler Newton matrix of the vortex
+    at the benchmark's dt/h), so the sync-free forms run with many CTAs in
+    flight and rows waiting on rows of other CTAs: forms with the same threads
+    per row agree bit for bit with the level form, the others within the
+    rounding of another summation order."""
+    n = 20000
+    V = [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0]
+    m = cp.PolyMesh.voronoi(cp.uniform_seeds(2, n, 10.0, 10.0), 10.0, 10.0, periodic=True)
+    eq = cp.Euler(ctx, m, 3, dirichlet=(cp.INIT_VORTEX, V), exact_jacobian=True)
+    u = eq.interp(cp.INIT_VORTEX, V)
+    J = eq.jacobian(u, 0.0, scale=-0.05 * (100000 / n) ** 0.5 * 0.435866521508459, add_mass=True, precision=prec)
+    P = _forms(ctx, monkeypatch, J, prec, [1, 2, 3, 4, 5, 6])
+    x = torch.randn(n * 40, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+    y = {f: p.solve(x.clone()) for f, p in P.items()}
+    assert torch.equal(y[1], y[2]) and torch.equal(y[4], y[2])
+    for f in (3, 5, 6):
+        assert rel(to_np(y[f]), to_np(y[2])) < (1e-12 if prec == cp.F64 else 1e-5)
+    # repeated applications reuse the flags with a new generation
+    assert torch.equal(P[4].solve(x.clone()), y[4])
+
+
+def test_sync_free_sweep_at_scale_matches_oracle(ctx, monkeypatch):
+    """30,000 block rows of 10x10 against the oracle's BlockILU0 solve."""
+    rp, cl, blocks = bsr(30000, 10, 11)
+    A = cp.BlockMatrix.from_host(ctx, rp, cl, blocks)
+    P = _forms(ctx, monkeypatch, A, cp.F64, [1, 4])
+    x = np.random.default_rng(5).standard_normal((len(rp) - 1) * 10)
+    want = oracle.precond_apply(2, rp, cl, blocks, x)
+    for p in P.values():
+        assert rel(to_np(p.solve(to_dev(x))), want) < 1e-11
