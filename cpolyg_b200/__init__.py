@@ -140,6 +140,21 @@ class PolyMesh:
             raise CpgError(st, "mesh construction failed")
         return cls(h)
 
+    def set_subtriangles(self, tri_ptr, tri_xy) -> None:
+        """Volume quadrature on these triangles (cell frame, 6 numbers each)
+        instead of the centroid fans, e.g. the reference's Triangle "zQq"
+        sub-triangulation; equations created afterwards use them."""
+        tp = np.ascontiguousarray(tri_ptr, dtype=np.int32)
+        tx = np.ascontiguousarray(tri_xy, dtype=np.float64).reshape(-1, 6)
+        if len(tp) != self.np + 1 or tp[-1] != len(tx):
+            raise ValueError("tri_ptr must have n_cells + 1 entries ending at the triangle count")
+        st = self._lib.cpg_mesh_set_subtriangles(self.h, _pi(tp), _pd(tx))
+        if st != 0:
+            raise CpgError(st, "sub-triangles do not tile the cells")
+        info = _capi.MeshInfo()
+        self._lib.cpg_mesh_get_info(self.h, C.byref(info))
+        self.n_tris = info.n_tris
+
     def export(self) -> dict:
         n, E, T = self.np, self.n_edges, self.n_tris
         out = dict(cell_ptr=np.zeros(n + 1, np.int32), poly_xy=np.zeros((E, 2)), vert_id=np.zeros(E, np.int32),

@@ -81,6 +81,7 @@ PROTOTYPES = {
     "cpg_seeds_uniform": (I, [C.c_uint64, I, D, D, PD]),
     "cpg_mesh_voronoi": (I, [PD, I, D, D, I, PI, PP]),
     "cpg_mesh_from_polygons": (I, [I, PI, PD, D, D, I, PI, PP]),
+    "cpg_mesh_set_subtriangles": (I, [P, PI, PD]),
     "cpg_mesh_destroy": (None, [P]),
     "cpg_mesh_get_info": (I, [P, C.POINTER(MeshInfo)]),
     "cpg_mesh_export": (I, [P, PI, PD, PI, PI, PD, PD, PI, PD]),

@@ -1,4 +1,6 @@
 // Context, error handling and the host-mesh part of the C ABI.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <new>
 
@@ -174,6 +176,40 @@ cpg_status cpg_mesh_from_polygons(int n, const int *cell_ptr, const double *poly
         return CPG_ERR_MESH;
     }
     *out = m;
+    return CPG_OK;
+}
+
+cpg_status cpg_mesh_set_subtriangles(cpg_mesh *mm, const int *tri_ptr, const double *tri_xy) {
+    if (!mm || !tri_ptr || !tri_xy) return CPG_ERR_INVALID_ARG;
+    Mesh &m = mm->m;
+    if (tri_ptr[0] != 0) return CPG_ERR_INVALID_ARG;
+    for (int i = 0; i < m.n; i++)
+        if (tri_ptr[i + 1] <= tri_ptr[i]) return CPG_ERR_INVALID_ARG;  // every cell needs a triangle
+    // the triangles of a cell must tile its polygon: same total area, and
+    // every vertex inside the cell's bounding box (cell-frame coordinates)
+    for (int i = 0; i < m.n; i++) {
+        const int s = m.cell_ptr[i], e = m.cell_ptr[i + 1];
+        double poly = 0.0;
+        for (int k = s; k < e; k++) {
+            const int k1 = k + 1 < e ? k + 1 : s;
+            poly += m.vxy[2 * k] * m.vxy[2 * k1 + 1] - m.vxy[2 * k1] * m.vxy[2 * k + 1];
+        }
+        poly *= 0.5;
+        double area = 0.0;
+        const double x0 = m.bb[4 * i], y0 = m.bb[4 * i + 1], w = m.bb[4 * i + 2], h = m.bb[4 * i + 3];
+        const double tol = 1e-9 * std::max(w, h);
+        for (int t = tri_ptr[i]; t < tri_ptr[i + 1]; t++) {
+            const double *T = tri_xy + 6 * (size_t)t;
+            for (int v = 0; v < 3; v++)
+                if (T[2 * v] < x0 - tol || T[2 * v] > x0 + w + tol || T[2 * v + 1] < y0 - tol ||
+                    T[2 * v + 1] > y0 + h + tol)
+                    return CPG_ERR_MESH;
+            area += 0.5 * std::fabs((T[2] - T[0]) * (T[5] - T[1]) - (T[4] - T[0]) * (T[3] - T[1]));
+        }
+        if (std::fabs(area - poly) > 1e-9 * std::fabs(poly)) return CPG_ERR_MESH;
+    }
+    m.tri_ptr.assign(tri_ptr, tri_ptr + m.n + 1);
+    m.tri.assign(tri_xy, tri_xy + 6 * (size_t)tri_ptr[m.n]);
     return CPG_OK;
 }
 

@@ -626,8 +626,8 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     bool timed = cudaMalloc(&tmp, N * sizeof(double)) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
                  cudaEventCreate(&e1) == cudaSuccess;
-    float best_ms[6] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
-    bool dropped[6] = {false, false, false, false, false, false};
+    float best_ms[8] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+    bool dropped[8] = {false, false, false, false, false, false, false, false};
     cpg_status st = CPG_OK;
     for (int rep = 0; rep < 2 && timed && st == CPG_OK; rep++)
         for (int c = 0; c < P->n_cand && st == CPG_OK; c++) {
@@ -689,20 +689,20 @@ void choose_form(cpg_precond *P, const char *env) {
         P->sweep_mode = 4;
         return;
     }
-    if (env && std::strncmp(env, "form", 4) == 0) {  // form1 .. form6
+    if (env && std::strncmp(env, "form", 4) == 0) {  // form1 .. form8
         const int f = std::atoi(env + 4);
         const bool needs_syncfree = f == 1 || f >= 4;
-        if (f >= 1 && f <= 6 && (!needs_syncfree || P->syncfree)) {
+        if (f >= 1 && f <= 8 && (!needs_syncfree || P->syncfree)) {
             P->sweep_mode = f;
             return;
         }
     }
     P->n_cand = 0;
-    if (P->syncfree) {
-        P->cand[P->n_cand++] = 1;
+    if (P->syncfree) {  // the TMA ring (1) and the widest direct rows (6) never won a size class
         P->cand[P->n_cand++] = 4;
         P->cand[P->n_cand++] = 5;
-        P->cand[P->n_cand++] = 6;
+        P->cand[P->n_cand++] = 7;
+        P->cand[P->n_cand++] = 8;
     }
     P->cand[P->n_cand++] = 2;
     if (rows_tunable(P->bl)) P->cand[P->n_cand++] = 3;
@@ -944,12 +944,14 @@ cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(col, h_col, sizeof(h_col), cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(order, h_order, sizeof(h_order), cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) st = cuda_fail(ctx, e, "sweep check setup");
-        // both sync-free forms; each must report its own wait running out
-        for (int form = 0; form < 2 && st == CPG_OK; form++) {
-            st = sweep_op(ctx, CPG_F64, 6, 1, order, rowptr, col, dbuf, dbuf + 36, MODE_FORWARD, flags, 1 + form,
-                          ctx->flag_dev + 4, ctx->flag_dev + 2, form);
+        // the three sync-free kernels (TMA ring, direct loads, scout warp);
+        // each must report its own wait running out
+        const int kinds[3] = {0, 1, 4};
+        for (int f = 0; f < 3 && st == CPG_OK; f++) {
+            st = sweep_op(ctx, CPG_F64, 6, 1, order, rowptr, col, dbuf, dbuf + 36, MODE_FORWARD, flags, 1 + f,
+                          ctx->flag_dev + 4, ctx->flag_dev + 2, kinds[f]);
             st = check_sweep_error(ctx, st);
-            if (st == CPG_ERR_TIMEOUT && form == 0) st = CPG_OK;  // go on to the second form
+            if (st == CPG_ERR_TIMEOUT && f < 2) st = CPG_OK;  // go on to the next kernel
             else if (st == CPG_OK) st = fail(ctx, CPG_ERR_INVALID_ARG, "a sweep wait did not report running out");
         }
     }

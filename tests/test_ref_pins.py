@@ -106,3 +106,61 @@ def test_subtriangulation_invisible_for_polynomials(p):
     u = np.random.default_rng(p).standard_normal(e_mine.ndof)
     bm, br = e_mine.assemble(u), e_ref.assemble(u)
     assert np.abs(bm - br).max() < 1e-12 * np.abs(br).max()
+
+
+def _ref_subtriangles(a, n):
+    ptr, poly = a["cell_ptr"], a["poly_xy"]
+    tri_ptr, tris = [0], []
+    for i in range(n):
+        T = ref_triangulate(poly[ptr[i]:ptr[i + 1]])
+        tris.append(T)
+        tri_ptr.append(tri_ptr[-1] + len(T))
+    return np.array(tri_ptr, np.int32), np.concatenate(tris)
+
+
+def test_library_takes_reference_subtriangles():
+    """cpg_mesh_set_subtriangles accepts the reference's Triangle "zQq"
+    sub-triangulation, exports it back, and rejects triangles that do not
+    tile the cells."""
+    n = 200
+    m = cp.PolyMesh.voronoi(cp.uniform_seeds(4, n, 10.0, 10.0), 10.0, 10.0, periodic=True)
+    a = m.export()
+    tp, tx = _ref_subtriangles(a, n)
+    bad = tx.copy()
+    bad[0, 2:4] = 0.5 * (bad[0, 0:2] + bad[0, 2:4])  # halve the first triangle
+    with pytest.raises(cp.CpgError):
+        m.set_subtriangles(tp, bad)
+    m.set_subtriangles(tp, tx)
+    b = m.export()
+    assert m.n_tris == len(tx)
+    assert np.array_equal(b["tri_ptr"], tp) and np.array_equal(b["tri_xy"].reshape(-1, 6), tx)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("deg", [2, 3])
+def test_euler_on_reference_subtriangles_matches_oracle(ctx, deg):
+    """The Euler residual and Jacobian integrated on the reference's Triangle
+    "zQq" sub-triangles (src/Triangulation.cpp:11-101) against the oracle on
+    the same triangles, <= 1e-12 relative: with them the library's Euler
+    results carry the reference's quadrature, not the centroid fans'."""
+    n = 300
+    V = [5.0, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0]
+    m = cp.PolyMesh.voronoi(cp.uniform_seeds(2, n, 10.0, 10.0), 10.0, 10.0, periodic=True)
+    a = m.export()
+    tp, tx = _ref_subtriangles(a, n)
+    m.set_subtriangles(tp, tx)
+    arrays = dict(a)
+    arrays["tri_ptr"], arrays["tri_xy"] = tp, tx
+    oe = oracle.Equation(oracle.Mesh(arrays), 2, deg, dkind=2, dparams=V)
+    ge = cp.Euler(ctx, m, deg, dirichlet=(cp.INIT_VORTEX, V))
+    u = oe.interp(2, V)
+    ud = __import__("torch").as_tensor(u).cuda().reshape(ge.np, ge.nc, ge.nb)
+    b_or = oe.assemble(u)
+    b_gpu = ge.assemble(ud).cpu().numpy().ravel()
+    assert np.abs(b_gpu - b_or).max() < 1e-12 * np.abs(b_or).max()
+    rp, cl, blk = oe.jacobian(u)
+    _, _, gblk = ge.jacobian(ud).export()
+    assert np.abs(gblk - blk).max() < 1e-12 * np.abs(blk).max()
+    # the fans give another quadrature of the non-polynomial Euler flux
+    oe_fan = oracle.Equation(oracle.Mesh(a), 2, deg, dkind=2, dparams=V)
+    assert np.abs(oe_fan.assemble(u) - b_or).max() > 1e-9 * np.abs(b_or).max()
