@@ -21,8 +21,10 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <type_traits>
 
 #include "internal.hpp"
+#include "tcgen05.cuh"
 
 using namespace cpg;
 
@@ -512,8 +514,267 @@ __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, con
     }
 }
 
+// ---------------------------------------------------------------------------
+// FP32 factors of 40x40 blocks on the 5th-generation tensor cores.  The same
+// three products per lower neighbour as k_ilu_factor (L_ji = A_ji D_i^{-1},
+// U_ij = D_i^{-1} A_ij, Ahat_jj -= L_ji A_ij), each a 64 x 40 x 40
+// tcgen05.mma of kind::tf32 (M padded from 40 to 64 with zero rows, five K
+// steps of 8) with the FP32 accumulator in TMEM.  SPLIT = 3 carries each FP32
+// operand as two TF32 parts and sums three products per K step, for about
+// FP32 accuracy; SPLIT = 1 is plain TF32.  One CTA (one warpgroup) per row:
+// all threads stage the operands into shared memory (core-matrix layout),
+// thread 0 issues the MMAs and commits them to an mbarrier, warps 0-2 read
+// the accumulators back (row m of an M = 64 accumulator sits in TMEM lane
+// m % 16 + 32 (m / 16)).  Ahat_jj = A_jj - sum L A is formed in FP64 in the
+// pivot's D^{-1} slot, which k_block_inverse then inverts in FP64 as before.
+// Every mbarrier wait is bounded; one that runs out sets flag[6], and the CTA
+// frees its TMEM and returns (the factorisation reports CPG_ERR_TIMEOUT).
+// ---------------------------------------------------------------------------
+namespace tcf {
+constexpr int BL = 40, M = 64, NT = 128, KSTEPS = BL / 8;
+constexpr int LBO = 128;                    // bytes between the 4-wide K chunks of a row group
+constexpr int SBO = (BL / 4) * LBO;         // bytes between 8-row groups (the whole K extent)
+constexpr int A_TILE = (M / 8) * SBO;       // 64 x 40 TF32: rows 40..63 stay zero
+constexpr int B_TILE = (BL / 8) * SBO;      // 40 x 40 TF32
+constexpr int PER = (BL * BL + NT - 1) / NT;
+constexpr uint32_t TMEM_COLS = 128;         // L at column 0, U at 40, sum(L A) at 80
+constexpr long long MAX_SPINS = 1LL << 24;  // mbarrier polls (>= 32 ns apart): > 0.5 s
+__host__ __device__ constexpr size_t smem_bytes(int split) {
+    return (size_t)(split == 3 ? 2 : 1) * (3 * A_TILE + 2 * B_TILE) + 64;
+}
+// byte offset of element (row r, K index k) in a K-major core-matrix tile
+__device__ __forceinline__ int off(int r, int k) { return (r >> 3) * SBO + (k >> 2) * LBO + (r & 7) * 16 + (k & 3) * 4; }
+__device__ __forceinline__ void put(unsigned char *hi, unsigned char *lo, int o, float x) {
+    if (lo) {
+        float h, l;
+        tc::split_tf32(x, h, l);
+        *(float *)(hi + o) = h;
+        *(float *)(lo + o) = l;
+    } else {
+        *(float *)(hi + o) = x;
+    }
+}
+// C (TMEM) = A * B over the five K steps; acc0: add to C's content
+template <int SPLIT>
+__device__ __forceinline__ void product(uint32_t c, const unsigned char *Ah, const unsigned char *Al,
+                                        const unsigned char *Bh, const unsigned char *Bl, bool acc0) {
+    constexpr uint32_t idesc = tc::idesc_tf32(M, BL);
+#pragma unroll
+    for (int s = 0; s < KSTEPS; s++) {
+        const uint32_t ko = (uint32_t)s * 2 * LBO;
+        const uint64_t ah = tc::sdesc(tc::saddr(Ah) + ko, LBO, SBO), bh = tc::sdesc(tc::saddr(Bh) + ko, LBO, SBO);
+        tc::mma_tf32(c, ah, bh, idesc, (acc0 || s > 0) ? 1u : 0u);
+        if (SPLIT == 3) {
+            const uint64_t al = tc::sdesc(tc::saddr(Al) + ko, LBO, SBO), bl = tc::sdesc(tc::saddr(Bl) + ko, LBO, SBO);
+            tc::mma_tf32(c, ah, bl, idesc, 1u);
+            tc::mma_tf32(c, al, bh, idesc, 1u);
+        }
+    }
+}
+// thread 0 waits (bounded) for the committed MMAs; the barrier hands the
+// outcome to every thread
+__device__ __forceinline__ bool wait_mma(uint64_t *bar, uint32_t parity, volatile int *s_ok) {
+    if (threadIdx.x == 0) {
+        long long spins = 0;
+        while (!tc::mbar_test(bar, parity)) {
+            if (++spins > MAX_SPINS) {
+                *s_ok = 0;
+                break;
+            }
+            if (spins > 64) __nanosleep(32);
+        }
+    }
+    __syncthreads();
+    return *s_ok != 0;
+}
+}  // namespace tcf
+
+template <int SPLIT>
+__global__ void __launch_bounds__(tcf::NT) k_ilu_factor_tc(const int *__restrict__ rows, const float *__restrict__ A,
+                                                          const int *__restrict__ diag_a, const int *__restrict__ lp_ptr,
+                                                          const int *__restrict__ lp_i, const int *__restrict__ lp_aji,
+                                                          const int *__restrict__ lp_aij, const int *__restrict__ lp_l,
+                                                          const int *__restrict__ lp_u, float *__restrict__ Lv,
+                                                          float *__restrict__ Uv, double *dinv,
+                                                          const int *__restrict__ dinv_idx, int *flag) {
+    using namespace tcf;
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr int H = SPLIT == 3 ? 2 : 1;  // tiles per operand
+    unsigned char *XA = smem, *DA = XA + H * A_TILE, *LA = DA + H * A_TILE;
+    unsigned char *DB = LA + H * A_TILE, *YB = DB + H * B_TILE;
+    uint64_t *bar = (uint64_t *)(YB + H * B_TILE);
+    uint32_t *s_tmem = (uint32_t *)(bar + 1);
+    volatile int *s_ok = (volatile int *)(s_tmem + 1);
+    auto lo = [&](unsigned char *t, int tile) -> unsigned char * { return SPLIT == 3 ? t + tile : nullptr; };
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int j = rows[blockIdx.x];
+    const int p0 = lp_ptr[j], p1 = lp_ptr[j + 1];
+    constexpr int BL2 = BL * BL;
+    // zero the A-operand tiles once: their rows 40..63 are never written
+    for (int o = tid; o < 3 * H * A_TILE / 16; o += NT) ((uint4 *)smem)[o] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) {
+        tc::mbar_init(bar, 1);
+        *s_ok = 1;
+    }
+    if (warp == 0) tc::tmem_alloc(s_tmem, TMEM_COLS);
+    tc::fence_smem_async();
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tbase = *s_tmem;
+    const uint32_t tL = tbase, tU = tbase + 40, tS = tbase + 80;
+    const uint32_t lrow = (uint32_t)(32 * warp) << 16;  // this warp's TMEM lane base
+    const int m = 16 * warp + lane;                      // accumulator row held by this thread
+    const bool row_ok = warp < 3 && lane < 16 && m < BL;
+    uint32_t parity = 0;
+    bool ok = true;
+    double rd[PER];
+    float rx[PER], ry[PER];
+    auto fetch = [&](int p) {
+        const double *d = dinv + (size_t)dinv_idx[lp_i[p]] * BL2;
+        const float *x = A + (size_t)lp_aji[p] * BL2, *y = A + (size_t)lp_aij[p] * BL2;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int o = tid + k * NT;
+            rd[k] = o < BL2 ? d[o] : 0.0;
+            rx[k] = o < BL2 ? x[o] : 0.0f;
+            ry[k] = o < BL2 ? y[o] : 0.0f;
+        }
+    };
+    if (p0 < p1) fetch(p0);
+    for (int p = p0; p < p1 && ok; p++) {
+        // operands: X = A_ji and D = D_i^{-1} as A tiles (row, K), D and
+        // Y = A_ij as B tiles (column, K); blocks are column-major
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int o = tid + k * NT;
+            if (o < BL2) {
+                const int r = o % BL, c = o / BL;
+                const float dv = (float)rd[k];
+                put(XA, lo(XA, A_TILE), off(r, c), rx[k]);
+                put(DA, lo(DA, A_TILE), off(r, c), dv);
+                put(DB, lo(DB, B_TILE), off(c, r), dv);
+                put(YB, lo(YB, B_TILE), off(c, r), ry[k]);
+            }
+        }
+        tc::fence_smem_async();
+        tc::fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after();
+            product<SPLIT>(tL, XA, lo(XA, A_TILE), DB, lo(DB, B_TILE), false);  // L_ji = A_ji D_i^{-1}
+            product<SPLIT>(tU, DA, lo(DA, A_TILE), YB, lo(YB, B_TILE), false);  // U_ij = D_i^{-1} A_ij
+            tc::commit(bar);
+        }
+        if (p + 1 < p1) fetch(p + 1);  // the next neighbour's blocks in flight during the products
+        ok = wait_mma(bar, parity, s_ok);
+        parity ^= 1;
+        if (!ok) break;
+        tc::fence_after();
+        if (warp < 3) {
+            float* Lg = Lv + (size_t)lp_l[p] * BL2;
+            float* Ug = Uv + (size_t)lp_u[p] * BL2;
+#pragma unroll
+            for (int cb = 0; cb < BL / 8; cb++) {
+                float v[8], w[8];
+                tc::tmem_ld8(tL + lrow + 8 * cb, v);
+                tc::tmem_ld8(tU + lrow + 8 * cb, w);
+                tc::tmem_wait_ld();
+                if (row_ok) {
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const int n = 8 * cb + q;
+                        Lg[(size_t)n * BL + m] = v[q];
+                        Ug[(size_t)n * BL + m] = w[q];
+                        put(LA, lo(LA, A_TILE), off(m, n), v[q]);  // L_ji as the A operand of the update
+                    }
+                }
+            }
+        }
+        tc::fence_smem_async();
+        tc::fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fence_after();
+            product<SPLIT>(tS, LA, lo(LA, A_TILE), YB, lo(YB, B_TILE), p > p0);  // sum_i L_ji A_ij
+            tc::commit(bar);
+        }
+        ok = wait_mma(bar, parity, s_ok);  // the tiles are free again
+        parity ^= 1;
+    }
+    // Ahat_jj = A_jj - sum_i L_ji A_ij, FP64, into the pivot's D^{-1} slot
+    double *dj = dinv + (size_t)dinv_idx[j] * BL2;
+    const float *ajj = A + (size_t)diag_a[j] * BL2;
+    if (ok && p0 == p1) {
+        for (int o = tid; o < BL2; o += NT) dj[o] = (double)ajj[o];
+    } else if (ok) {
+        tc::fence_after();
+        if (warp < 3) {
+#pragma unroll
+            for (int cb = 0; cb < BL / 8; cb++) {
+                float v[8];
+                tc::tmem_ld8(tS + lrow + 8 * cb, v);
+                tc::tmem_wait_ld();
+                if (row_ok) {
+#pragma unroll
+                    for (int q = 0; q < 8; q++) {
+                        const size_t o = (size_t)(8 * cb + q) * BL + m;
+                        dj[o] = (double)ajj[o] - (double)v[q];
+                    }
+                }
+            }
+        }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fence_after();
+        tc::tmem_dealloc(tbase, TMEM_COLS);
+    }
+    if (!ok && tid == 0) atomicExch(flag + 6, 1);
+}
+
+// the tensor-core factor applies to FP32 matrices and factors of 40x40
+// blocks; CPG_FACTOR_TC=0 selects the FP64-DMMA products instead, =1 plain
+// TF32 (one pass), default three TF32 passes
+int factor_tc_mode() {
+    const char *e = std::getenv("CPG_FACTOR_TC");
+    if (!e) return 3;
+    const int v = std::atoi(e);
+    return v == 0 ? 0 : (v == 1 ? 1 : 3);
+}
+
+template <int SPLIT>
+cpg_status launch_factor_tc(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
+    // dynamic shared memory of at least 57 KB keeps at most 4 CTAs (4 x 128
+    // TMEM columns) on an SM, so no TMEM allocation ever waits for another CTA
+    const size_t smem = std::max<size_t>(tcf::smem_bytes(SPLIT), 57 * 1024);
+    CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor_tc<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_ilu_factor_tc<SPLIT><<<nrows, tcf::NT, smem, ctx->stream>>>(
+        rows, (const float *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
+        P->lp_u_d, (float *)P->L_vals, (float *)P->U_vals, P->dinv64, P->dinv_idx_d, ctx->flag_dev);
+    CPG_TRY(launched(ctx, "ilu factor kernel (tcgen05 tf32)"));
+    // pivot-block inverses in FP64, as on the other paths
+    constexpr int BL = tcf::BL;
+    const size_t b2 = (size_t)BL * BL;
+    const size_t per_warp = (b2 + 8 * (size_t)(BL - 8) + BL) * sizeof(double);
+    const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
+    const size_t ismem = per_warp * wpb;
+    if ((int)ismem > 48 * 1024)
+        CPG_CUDA(ctx, cudaFuncSetAttribute(k_block_inverse<float, 40>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)ismem));
+    k_block_inverse<float, 40><<<(nrows + wpb - 1) / wpb, 32 * wpb, ismem, ctx->stream>>>(
+        BL, nrows, rows, (float *)P->U_vals, P->U_rowptr_d, P->dinv64, P->dinv_idx_d, ctx->flag_dev);
+    return launched(ctx, "pivot block inverse kernel");
+}
+
 template <class TA, class TS, int BLC>
 cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrows, const int *rows) {
+    if constexpr (std::is_same<TA, float>::value && std::is_same<TS, float>::value && BLC == 40) {
+        const int mode = factor_tc_mode();
+        if (mode == 3) return launch_factor_tc<3>(ctx, P, A, nrows, rows);
+        if (mode == 1) return launch_factor_tc<1>(ctx, P, A, nrows, rows);
+    }
     const int BL = P->bl;
     const int ld = (BLC > 0 && BLC % 8 == 0) ? BL + 4 : BL;  // padded blocks on the DMMA path
     const size_t smem = 5 * (size_t)BL * ld * sizeof(double) + 16;
@@ -905,12 +1166,14 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A) 
     if (A->n_rows != P->n || A->bl != P->bl) return fail(ctx, CPG_ERR_INVALID_ARG, "matrix does not fit preconditioner");
     const int init[2] = {0, INT_MAX};
     CPG_CUDA(ctx, cudaMemcpyAsync(ctx->flag_dev, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    CPG_CUDA(ctx, cudaMemsetAsync(ctx->flag_dev + 6, 0, sizeof(int), ctx->stream));
     const int nlev = (int)P->lptr.size() - 1;
     for (int l = 0; l < nlev; l++)
         CPG_TRY(factor_level(ctx, P, A, P->lptr[l + 1] - P->lptr[l], P->lrows_d + P->lptr[l]));
-    int flag[2];
+    int flag[7];
     CPG_CUDA(ctx, cudaMemcpyAsync(flag, ctx->flag_dev, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (flag[6]) return fail(ctx, CPG_ERR_TIMEOUT, "a tensor-core product of the factorisation did not complete");
     if (flag[0]) return fail(ctx, CPG_ERR_SINGULAR_BLOCK, "singular pivot block at row " + std::to_string(flag[1]));
     return CPG_OK;
 }

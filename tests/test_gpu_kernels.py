@@ -198,6 +198,27 @@ def test_gmres_vs_oracle(ctx, pc):
     assert np.linalg.norm(dense @ to_np(xg) - b) < 1e-9 * np.linalg.norm(b)
 
 
+@pytest.mark.parametrize("mode,tol", [("3", 2e-6), ("1", 2e-3), ("0", 1e-6)])
+def test_fp32_ilu_factor_tensor_core_products(ctx, monkeypatch, mode, tol):
+    """FP32 factors of 40x40 blocks: the block products run on tcgen05
+    kind::tf32 MMAs (mode 3: three TF32 passes, about FP32 accuracy; mode 1:
+    one pass) or on FP64 DMMA (mode 0).  Factors and one application against
+    the oracle's FP64 factorisation; pivots stay FP64."""
+    monkeypatch.setenv("CPG_FACTOR_TC", mode)
+    bl = 40
+    rp, cl, blocks = random_bsr(60, bl, seed=21)
+    A32 = cp.BlockMatrix.from_host(ctx, rp, cl, blocks, precision=cp.F32)
+    P = cp.BlockILU0(A32, precision=cp.F32)
+    b32 = blocks.astype(np.float32).astype(np.float64)  # the FP32 matrix the GPU sees
+    dd, (lr, lc, lb), (ur, uc, ub), sing = oracle.ilu0(rp, cl, b32)
+    gdd, (glr, glc, glb), (gur, guc, gub) = P.export(len(lc), len(uc))
+    assert rel(glb, lb) < tol and rel(gub, ub) < tol and rel(gdd, dd) < tol
+    x = np.random.default_rng(3).standard_normal((len(rp) - 1) * bl)
+    xd = to_dev(x)
+    P.solve(xd)
+    assert rel(to_np(xd), oracle.precond_apply(2, rp, cl, b32, x)) < 10 * tol
+
+
 def test_fgmres_solves(ctx):
     bl = 40
     rp, cl, blocks = random_bsr(60, bl, seed=13)
