@@ -178,13 +178,14 @@ def peaks() -> dict:
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def profiled_traffic(name: str):
-    """dram bytes per launch recorded from an ncu capture in profiles/"""
+def profiled_traffic(name: str, key: str = "traffic_bytes_per_launch"):
+    """dram bytes per launch (or per application) recorded from an ncu
+    capture in profiles/"""
     p = os.path.join(ROOT, "profiles", name)
     if not os.path.exists(p):
         return None
     for ln in open(p):
-        if ln.startswith("traffic_bytes_per_launch:"):
+        if ln.startswith(key + ":"):
             try:
                 return float(ln.split(":", 1)[1].split()[0])
             except ValueError:
@@ -435,7 +436,7 @@ def roofline(a, cp, ctx, eq, u, t, stream):
     prec_sw = "FP32" if s_p == 4 else "FP64"
     kname = {1: "k_sweep (TMA ring)", 4: "k_sweep_direct", 5: "k_sweep_direct (2x rows)",
              6: "k_sweep_direct (4x rows)", 2: "k_rows per level", 3: "k_rows per level (wide)"}.get(form, "sweep")
-    traffic = profiled_traffic(f"sweep_direct_{prec_sw.lower()}_bl{bl}_100k.md")
+    traffic = profiled_traffic(f"sweep_direct_{prec_sw.lower()}_bl{bl}_100k.md", "traffic_bytes_per_apply")
     roof = {"kernel": f"{kname}: ILU(0) apply, forward + backward sweep, {bl}x{bl} {prec_sw} factors "
                       f"(sweep form {form})",
             "bound": "hbm", "achieved": ach_sw, "peak": pk["hbm_gbs"], "unit": "GB/s",

@@ -654,163 +654,8 @@ cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, co
     return launched(ctx, "sync-free sweep kernel (direct)");
 }
 
-// ---------------------------------------------------------------------------
-// Direct loads with a scout warp.  The direct form's rows start with a chain
-// of dependent loads (claim counter -> row index -> row pointer -> block
-// columns) and then fetch their values from HBM, all on the sweep's critical
-// path, which is what bounds it when a level holds few rows per SM (small
-// meshes, FP32 factors).  Here one extra warp per CTA runs a row ahead of the
-// TPR consumer threads: while they stream row r, it claims row r+1, resolves
-// its index, extent and block columns into shared memory, and issues an L2
-// bulk prefetch (cp.async.bulk.prefetch.L2, no multicast) of the values of
-// the row `pf` places later in claim order -- a row some CTA will claim about
-// one row-time later -- so the consumers stream from L2.  A CTA holds at most
-// the row it works on and the next claimed one, in claim order, so the
-// progress argument of the direct form holds.  The consumers keep the
-// direct form's threads per row and element order: the same bits.
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
-
-template <class T, int BL, int TPR>
-__global__ void __launch_bounds__(TPR + 32, 2048 / (TPR + 32))
-    k_sweep_scout(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
-                  const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags, int gen,
-                  int *counter, int *err, int pf) {
-    constexpr int VEC = SweepShape<T, BL>::VEC;
-    constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
-    static_assert(BL2 * sizeof(T) % 16 == 0, "bulk prefetch sizes are multiples of 16 bytes");
-    __shared__ int s_meta[2][4];  // claim index q, row i, first block k0, blocks in the row
-    __shared__ int s_col[2][SWEEP_MAXB];
-    __shared__ double red[G][BL];
-    const int tid = threadIdx.x, lane = tid & 31;
-    const bool is_scout = tid >= TPR;
-    const int first_dep = (mode == MODE_BACKWARD) ? 1 : 0;  // the backward row's block 0 is D^{-1}_i
-    // claim the next row into slot `slot` and prefetch the values of the row
-    // pf claims later (lane 0 follows the claimed row, lane 1 the prefetched one)
-    auto scout = [&](int slot) {
-        int qn = 0;
-        if (lane == 0) qn = atomicAdd(counter, 1);
-        qn = __shfl_sync(0xffffffffu, qn, 0);
-        const int qq = lane == 0 ? qn : qn + pf;
-        int ii = 0, ka = 0, kb = 0;
-        if (lane < 2 && qq < n) {
-            ii = order[qq];
-            ka = rowptr[ii];
-            kb = rowptr[ii + 1];
-        }
-        const int i0 = __shfl_sync(0xffffffffu, ii, 0), a0 = __shfl_sync(0xffffffffu, ka, 0);
-        const int n0 = __shfl_sync(0xffffffffu, kb - ka, 0);
-        const int a1 = __shfl_sync(0xffffffffu, ka, 1), n1 = __shfl_sync(0xffffffffu, kb - ka, 1);
-        if (qn < n && lane < n0 && lane < SWEEP_MAXB) s_col[slot][lane] = col[a0 + lane];
-        if (qn + pf < n && pf > 0 && lane < n1)
-            prefetch_l2(vals + (size_t)(a1 + lane) * BL2, (uint32_t)(BL2 * sizeof(T)));
-        if (lane == 0) {
-            s_meta[slot][0] = qn;
-            s_meta[slot][1] = i0;
-            s_meta[slot][2] = a0;
-            s_meta[slot][3] = n0;
-        }
-    };
-    if (is_scout) scout(0);
-    __syncthreads();
-    const int e0 = tid * VEC;
-    const int r0 = e0 % BL, g = e0 / BL;
-    const double s0 = (mode == MODE_FORWARD) ? -1.0 : 1.0;
-    const double sr = -1.0;
-    for (int cur = 0;; cur ^= 1) {
-        const int q = s_meta[cur][0];
-        if (q >= n) break;
-        const int i = s_meta[cur][1];
-        if (is_scout) {
-            scout(cur ^ 1);
-        } else {
-            const int k0 = s_meta[cur][2], nraw = s_meta[cur][3];
-            const int nblk = nraw > SWEEP_MAXB ? 0 : nraw;  // the host admits no longer rows
-            if (tid == 0 && nraw > SWEEP_MAXB) atomicExch(err, 3);
-            for (int b = tid; b < nblk; b += TPR) {
-                if (b >= first_dep) {
-                    const int j = s_col[cur][b];
-                    long long spins = 0;
-                    while (ld_acquire(flags + j) != gen) {
-                        if (++spins > SWEEP_MAX_SPINS || ((spins & 255) == 0 && ld_acquire(err) != 0)) {
-                            atomicExch(err, 1);
-                            break;
-                        }
-                        __nanosleep(64);
-                    }
-                }
-            }
-            consumers_sync(TPR);
-            double acc[VEC];
-#pragma unroll
-            for (int v = 0; v < VEC; v++) acc[v] = 0.0;
-            const T *base = vals + (size_t)k0 * BL2;
-            const int E = nblk * BL2;
-            int blk = e0 / BL2, within = e0 % BL2;
-#pragma unroll 4
-            for (int e = e0; e < E; e += S) {
-                const int c = within / BL;
-                double a[VEC];
-                VecLoad<T, VEC>::ld(base + e, a);
-                // values published during this sweep: read through L2, not L1
-                const double xv = __ldcg(x + (size_t)s_col[cur][blk] * BL + c) * (blk == 0 ? s0 : sr);
-#pragma unroll
-                for (int v = 0; v < VEC; v++) acc[v] += a[v] * xv;
-                within += S;
-                while (within >= BL2) {
-                    within -= BL2;
-                    blk++;
-                }
-            }
-#pragma unroll
-            for (int v = 0; v < VEC; v++) red[g][r0 + v] = acc[v];
-            consumers_sync(TPR);
-            if (tid < BL) {
-                double sum = 0.0;
-#pragma unroll
-                for (int qq = 0; qq < G; qq++) sum += red[qq][tid];
-                double *xi = x + (size_t)i * BL;
-                if (mode == MODE_FORWARD) sum = __ldcg(xi + tid) + sum;
-                __stcg(xi + tid, sum);
-            }
-        }
-        __syncthreads();  // the row's stores are done and the next row's slot is filled
-        if (tid == 0) {
-            __threadfence();
-            st_release(flags + i, gen);
-        }
-    }
-}
-
-template <class T, int BL, int TPR>
-cpg_status launch_sweep_scout_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
-                                  const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
-    static int per_sm[64] = {};
-    const bool cacheable = ctx->device >= 0 && ctx->device < 64;
-    int occ = cacheable ? per_sm[ctx->device] : 0;
-    if (!occ) {
-        CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep_scout<T, BL, TPR>, TPR + 32, 0));
-        if (cacheable) per_sm[ctx->device] = occ;
-    }
-    const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
-    // prefetch distance in claim order: about half of the rows the grid works
-    // on at once, i.e. rows that are claimed about half a row-time later
-    static const int pf_env = [] {
-        const char *e = std::getenv("CPG_SWEEP_PREFETCH");
-        return e ? std::atoi(e) : -1;
-    }();
-    const int pf = pf_env >= 0 ? pf_env : std::max(1, grid / 2);
-    CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
-    k_sweep_scout<T, BL, TPR><<<grid, TPR + 32, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags,
-                                                                 gen, counter, err, pf);
-    return launched(ctx, "sync-free sweep kernel (scout warp)");
-}
-
 // kind 0: TMA ring; kinds 1, 2, 3: direct loads with 1, 2 or 4 times the
-// consumer threads per row (the level form's variants 0, 1, 2); kinds 4, 5:
-// direct loads with a scout warp, 1 or 2 times the consumer threads
+// consumer threads per row (the level form's variants 0, 1, 2)
 template <class T>
 cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, const int *rowptr, const int *col,
                           const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err,
@@ -829,12 +674,6 @@ cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, con
             case 3:                                                                                             \
                 return launch_sweep_direct_cfg<T, BLV, 4 * CT>(ctx, nrows, order, rowptr, col, vals, x, mode,    \
                                                                flags, gen, counter, err);                       \
-            case 4:                                                                                             \
-                return launch_sweep_scout_cfg<T, BLV, CT>(ctx, nrows, order, rowptr, col, vals, x, mode, flags,  \
-                                                          gen, counter, err);                                   \
-            case 5:                                                                                             \
-                return launch_sweep_scout_cfg<T, BLV, 2 * CT>(ctx, nrows, order, rowptr, col, vals, x, mode,     \
-                                                              flags, gen, counter, err);                        \
             default:                                                                                            \
                 return launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen,       \
                                                 counter, err);                                                  \

@@ -96,10 +96,9 @@ struct cpg_precond {
     // the candidates), 1 = sync-free with a TMA ring, 2 = level sweeps with
     // the sync-free forms' threads per row (bitwise the same result as 1 and
     // 4), 3 = level sweeps with the widest rows, 4 / 5 / 6 = sync-free with
-    // direct loads and 1 / 2 / 4 times those threads per row, 7 / 8 = the
-    // direct form with a scout warp (1 / 2 times those threads per row)
+    // direct loads and 1 / 2 / 4 times those threads per row
     mutable int sweep_mode = 2;
-    int n_cand = 0, cand[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int n_cand = 0, cand[6] = {0, 0, 0, 0, 0, 0};
     int form_key = -1;  // process-wide key of the decision (block size, precision, size class)
     int64_t nnzL = 0, nnzU = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }

@@ -734,12 +734,15 @@ __global__ void __launch_bounds__(tcf::NT) k_ilu_factor_tc(const int *__restrict
     if (!ok && tid == 0) atomicExch(flag + 6, 1);
 }
 
-// the tensor-core factor applies to FP32 matrices and factors of 40x40
-// blocks; CPG_FACTOR_TC=0 selects the FP64-DMMA products instead, =1 plain
-// TF32 (one pass), default three TF32 passes
+// The tensor-core factor applies to FP32 matrices and factors of 40x40
+// blocks, on request: CPG_FACTOR_TC=3 (three TF32 passes) or =1 (one pass).
+// The default keeps the FP64-DMMA products: the pivot update Ahat_jj -=
+// sum L_ji A_ij of the stiff Newton matrix cancels heavily, and TF32-class
+// products with an FP32 accumulator leave pivots that double FGMRES's
+// iterations (three passes) or stall it (one pass).
 int factor_tc_mode() {
     const char *e = std::getenv("CPG_FACTOR_TC");
-    if (!e) return 3;
+    if (!e) return 0;
     const int v = std::atoi(e);
     return v == 0 ? 0 : (v == 1 ? 1 : 3);
 }
@@ -950,10 +953,10 @@ void choose_form(cpg_precond *P, const char *env) {
         P->sweep_mode = 4;
         return;
     }
-    if (env && std::strncmp(env, "form", 4) == 0) {  // form1 .. form8
+    if (env && std::strncmp(env, "form", 4) == 0) {  // form1 .. form6
         const int f = std::atoi(env + 4);
         const bool needs_syncfree = f == 1 || f >= 4;
-        if (f >= 1 && f <= 8 && (!needs_syncfree || P->syncfree)) {
+        if (f >= 1 && f <= 6 && (!needs_syncfree || P->syncfree)) {
             P->sweep_mode = f;
             return;
         }
@@ -962,8 +965,6 @@ void choose_form(cpg_precond *P, const char *env) {
     if (P->syncfree) {  // the TMA ring (1) and the widest direct rows (6) never won a size class
         P->cand[P->n_cand++] = 4;
         P->cand[P->n_cand++] = 5;
-        P->cand[P->n_cand++] = 7;
-        P->cand[P->n_cand++] = 8;
     }
     P->cand[P->n_cand++] = 2;
     if (rows_tunable(P->bl)) P->cand[P->n_cand++] = 3;
@@ -1207,14 +1208,13 @@ cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(col, h_col, sizeof(h_col), cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess) e = cudaMemcpyAsync(order, h_order, sizeof(h_order), cudaMemcpyHostToDevice, ctx->stream);
         if (e != cudaSuccess) st = cuda_fail(ctx, e, "sweep check setup");
-        // the three sync-free kernels (TMA ring, direct loads, scout warp);
-        // each must report its own wait running out
-        const int kinds[3] = {0, 1, 4};
-        for (int f = 0; f < 3 && st == CPG_OK; f++) {
+        // both sync-free kernels (TMA ring, direct loads); each must report
+        // its own wait running out
+        for (int f = 0; f < 2 && st == CPG_OK; f++) {
             st = sweep_op(ctx, CPG_F64, 6, 1, order, rowptr, col, dbuf, dbuf + 36, MODE_FORWARD, flags, 1 + f,
-                          ctx->flag_dev + 4, ctx->flag_dev + 2, kinds[f]);
+                          ctx->flag_dev + 4, ctx->flag_dev + 2, f);
             st = check_sweep_error(ctx, st);
-            if (st == CPG_ERR_TIMEOUT && f < 2) st = CPG_OK;  // go on to the next kernel
+            if (st == CPG_ERR_TIMEOUT && f == 0) st = CPG_OK;  // go on to the next kernel
             else if (st == CPG_OK) st = fail(ctx, CPG_ERR_INVALID_ARG, "a sweep wait did not report running out");
         }
     }

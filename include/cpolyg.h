@@ -342,23 +342,20 @@ void cpg_precond_destroy(cpg_precond *P);
  * threads per row (bitwise the same result as 1), 3 = one launch per level
  * with the widest rows (another summation order), 4 / 5 / 6 = sync-free
  * with direct loads and 1 / 2 / 4 times form 1's threads per row (4 sums
- * as 1), 7 / 8 = forms 4 / 5 with a scout warp that claims the next row
- * ahead and prefetches rows into L2 (7 sums as 1), 0 = not decided yet: the
+ * as 1), 0 = not decided yet: the
  * first application times the candidates on a scratch copy of its vector,
  * then applies the fastest, and the decision holds for every ILU(0)
  * preconditioner of the process with the same block size, precision and
  * size class.  CPG_ILU_SWEEP=syncfree, =syncfree_direct, =levels,
  * =levels_wide or =form<N> in the environment when the preconditioner is
- * created forces a form; CPG_SWEEP_PREFETCH=<rows> sets the scout's prefetch
- * distance in claim order (default: half the CTAs of the sweep's grid).  No counterpart in the reference (its sweeps are sequential
+ * created forces a form.  No counterpart in the reference (its sweeps are sequential
  * loops, Preconditioners.cpp:125-158).                                      */
 int cpg_precond_sweep_form(const cpg_precond *P);
 /* Failure-detection check of the sync-free sweeps: runs, for each of the
- * three sync-free kernels (TMA ring, direct loads, scout warp), a one-row
- * sweep whose dependency is never published, so the row's bounded wait runs
- * out (a few seconds each); returns CPG_ERR_TIMEOUT when all of them
- * reported it, and leaves the context usable.  No counterpart in the
- * reference.                                                                */
+ * two sync-free kernels (TMA ring, direct loads), a one-row sweep whose
+ * dependency is never published, so the row's bounded wait runs out (a few
+ * seconds each); returns CPG_ERR_TIMEOUT when both reported it, and leaves
+ * the context usable.  No counterpart in the reference.                     */
 cpg_status cpg_debug_sweep_timeout(cpg_ctx *ctx);
 /* ILU(0) level schedule (row lists by level), for checks:
  *   lower_ptr[levels_lower+1], lower_rows[n], upper_ptr[...], upper_rows[n] */
