@@ -155,6 +155,12 @@ class PolyMesh:
         self._lib.cpg_mesh_get_info(self.h, C.byref(info))
         self.n_tris = info.n_tris
 
+    def gnuplot(self, path: str = "plt/edges.gnu") -> None:
+        """PolyMesh::gnuplot: polygon outlines as gnuplot text."""
+        st = self._lib.cpg_mesh_write_gnuplot(self.h, str(path).encode())
+        if st != 0:
+            raise CpgError(st, f"cannot write {path}")
+
     def export(self) -> dict:
         n, E, T = self.np, self.n_edges, self.n_tris
         out = dict(cell_ptr=np.zeros(n + 1, np.int32), poly_xy=np.zeros((E, 2)), vert_id=np.zeros(E, np.int32),
@@ -284,6 +290,12 @@ class Equation:
         self.ctx.check(self._lib.cpg_l2norm(self.ctx.h, self.h, C.c_void_p(_ptr(u)), _pd(out)))
         return out[: self.nc].copy()
 
+    def gnuplot(self, u, path: str) -> None:
+        """MeshFn::gnuplot: field values at the 3-point rule of every
+        sub-triangle, as gnuplot text."""
+        self.ctx.check(self._lib.cpg_field_write_gnuplot(self.ctx.h, self.h, self.msh.h, C.c_void_p(_ptr(u)),
+                                                         str(path).encode()))
+
     def L2Error(self, u, kind: int, params, t: float = 0.0) -> np.ndarray:
         """MeshFn::L2Error (src/MeshFn.cpp:283-296) against the analytic field
         (kind, params) at time t, per component."""
@@ -345,6 +357,10 @@ class BlockMatrix:
         vals = np.zeros((self.nb, self.bl, self.bl))
         self.ctx.check(self._lib.cpg_bsr_export(self.ctx.h, self.h, _pi(rp), _pi(cl), _pd(vals)))
         return rp, cl, vals
+
+    def spy(self, path: str) -> None:
+        """BlockMatrix::spy: nonzero entries as gnuplot text."""
+        self.ctx.check(self._lib.cpg_bsr_write_spy(self.ctx.h, self.h, str(path).encode()))
 
     def matvec(self, x):
         import torch

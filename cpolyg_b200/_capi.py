@@ -83,6 +83,9 @@ PROTOTYPES = {
     "cpg_mesh_from_polygons": (I, [I, PI, PD, D, D, I, PI, PP]),
     "cpg_mesh_set_subtriangles": (I, [P, PI, PD]),
     "cpg_mesh_destroy": (None, [P]),
+    "cpg_mesh_write_gnuplot": (I, [P, C.c_char_p]),
+    "cpg_field_write_gnuplot": (I, [P, P, P, P, C.c_char_p]),
+    "cpg_bsr_write_spy": (I, [P, P, C.c_char_p]),
     "cpg_mesh_get_info": (I, [P, C.POINTER(MeshInfo)]),
     "cpg_mesh_export": (I, [P, PI, PD, PI, PI, PD, PD, PI, PD]),
     "cpg_mesh_pattern": (I, [P, PI, PI, PI64]),

@@ -18,7 +18,7 @@ BUILD = os.path.join(HERE, "_build")
 LIBDIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIBDIR, "libcpolyg_b200.so")
 
-CU_SOURCES = ["core.cu", "equation.cu", "bsr.cu", "precond.cu", "krylov.cu", "stepper.cu"]
+CU_SOURCES = ["core.cu", "equation.cu", "bsr.cu", "precond.cu", "krylov.cu", "stepper.cu", "output.cu"]
 CXX_SOURCES = ["mesh.cpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -446,6 +446,23 @@ cpg_status cpg_step(cpg_ctx *ctx, cpg_stepper *s, double *u_dev, double dt,
 cpg_status cpg_step_host(cpg_ctx *ctx, cpg_stepper *s, double *u_host,
                          double dt, double t, cpg_step_stats *stats);
 
+/* ------------------------------------------------------------------------ */
+/* gnuplot text output (visual cross-checks; host files)                    */
+/* ------------------------------------------------------------------------ */
+/* PolyMesh::gnuplot (src/PolyMesh.cpp:221-241): per cell "# polygon number
+ * i", its vertices with the first repeated, a blank line.  Coordinates are
+ * the cell's own frame, so periodic cells are not cut at the domain edge.   */
+cpg_status cpg_mesh_write_gnuplot(const cpg_mesh *m, const char *path);
+/* MeshFn::gnuplot (src/MeshFn.cpp:161-207): one line "x y u_0 .. u_nc-1" per
+ * point of the 3-point triangle rule on every sub-triangle of every cell;
+ * the field is evaluated on the device.  m must be the equation's mesh.    */
+cpg_status cpg_field_write_gnuplot(cpg_ctx *ctx, const cpg_equation *eq,
+                                   const cpg_mesh *m, const double *u_dev,
+                                   const char *path);
+/* BlockMatrix::spy (src/BlockMatrix.cpp:318-349): one line "row col value"
+ * per entry with |value| > 1e-10.                                            */
+cpg_status cpg_bsr_write_spy(cpg_ctx *ctx, const cpg_bsr *A, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

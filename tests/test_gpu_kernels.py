@@ -113,6 +113,47 @@ def test_l2_error(ctx, name, deg, kind, params, t):
     assert np.abs(ge.L2Error(ui, kind, params, t) - oe.l2error(to_np(ui), kind, params, t)).max() < 1e-12 * scale
 
 
+def test_field_and_matrix_gnuplot_files(ctx, tmp_path):
+    """MeshFn::gnuplot: one line per point of the 3-point rule on every
+    sub-triangle, values (evaluated on the device) equal to the oracle's
+    Leg2D at those points; BlockMatrix::spy: every entry above 1e-10."""
+    ge, oe, a = equations(ctx, "euler", 2, n=120, periodic=True, width=10.0)
+    u = oe.interp(cp.INIT_VORTEX, [5.0, 5.0, 5.0, 1, 1, 1.4, 10, 10])
+    ud = to_dev(u).reshape(ge.np, ge.nc, ge.nb)
+    path = tmp_path / "u.gnu"
+    ge.gnuplot(ud, str(path))
+    rows = np.array([[float(v) for v in ln.split("\t")] for ln in path.read_text().splitlines()])
+    tri = a["tri_xy"].reshape(-1, 6)
+    q = np.array([[1 / 6, 1 / 6], [1 / 6, 2 / 3], [2 / 3, 1 / 6]])  # the 3-point rule's (a, b)
+    assert rows.shape == (3 * len(tri), 2 + ge.nc)
+    k = 0
+    nb = ge.nb
+    for i in range(ge.np):
+        x0, y0, w, h = a["bb"][i]
+        for t in range(a["tri_ptr"][i], a["tri_ptr"][i + 1]):
+            T = tri[t]
+            for qa, qb in q:
+                x = T[0] * (1 - qa - qb) + T[2] * qa + T[4] * qb
+                y = T[1] * (1 - qa - qb) + T[3] * qa + T[5] * qb
+                assert abs(rows[k, 0] - x) <= 1e-5 * max(1.0, abs(x)) and abs(rows[k, 1] - y) <= 1e-5 * max(1.0, abs(y))
+                for c in range(ge.nc):
+                    want = oracle.leg2d(2 * (x - x0) / w - 1, 2 * (y - y0) / h - 1, 3, u[i * ge.bl + c * nb:][:nb])
+                    assert abs(rows[k, 2 + c] - want) <= 1e-12 * max(1.0, abs(want))
+                k += 1
+    # spy of the Jacobian
+    J = ge.jacobian(ud)
+    rp, cl, blk = J.export()
+    J.spy(str(tmp_path / "J.spy"))
+    got = np.loadtxt(tmp_path / "J.spy")
+    bl = ge.bl
+    want = [(i * bl + ii, cl[k] * bl + jj, blk[k][jj, ii]) for i in range(len(rp) - 1) for k in range(rp[i], rp[i + 1])
+            for ii in range(bl) for jj in range(bl) if abs(blk[k][jj, ii]) > 1e-10]
+    assert got.shape == (len(want), 3)
+    w = np.array(want)
+    assert np.array_equal(got[:, :2], w[:, :2])
+    assert np.allclose(got[:, 2], w[:, 2], rtol=1e-5)
+
+
 BLS = [1, 3, 4, 6, 7, 10, 12, 24, 40, 48]
 
 

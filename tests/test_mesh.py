@@ -157,3 +157,20 @@ def test_benchmark_mesh_pattern_and_levels_match_oracle():
     assert len(cl) == 100000 + len(a["edge_nbr"])
     for x, y in zip(cp.pattern_levels(rp, cl), oracle.levels(rp, cl)):
         assert np.array_equal(x, y)
+
+
+def test_mesh_gnuplot_file(tmp_path):
+    """PolyMesh::gnuplot format: "# polygon number i", the vertices with the
+    first one repeated, a blank line; the cell's own frame."""
+    m, a, _ = mesh(300, True, 1.0)
+    path = tmp_path / "edges.gnu"
+    m.gnuplot(str(path))
+    blocks = path.read_text().strip("\n").split("\n\n")
+    assert len(blocks) == 300
+    for i, b in enumerate(blocks):
+        lines = b.split("\n")
+        assert lines[0] == f"# polygon number {i}"
+        pts = np.array([[float(v) for v in ln.split("\t")] for ln in lines[1:]])
+        P = a["poly_xy"][a["cell_ptr"][i]:a["cell_ptr"][i + 1]]
+        assert len(pts) == len(P) + 1 and np.array_equal(pts[0], pts[-1])
+        assert np.allclose(pts[:-1], P, rtol=1e-5, atol=1e-6)
