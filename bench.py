@@ -54,7 +54,8 @@ def parse():
                          "factors (FP64 operator, FP32 preconditioner)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="dirk3", choices=["dirk3", "irk", "serve"],
+    ap.add_argument("--systems", type=int, default=16, help="batch: independent systems per batched solve")
+    ap.add_argument("--workload", default="dirk3", choices=["dirk3", "irk", "serve", "batch"],
                     help="dirk3: the 100k-cell vortex (default); irk: 2-stage Radau IIA, 500k cells, walls/inflow/"
                          "outflow, stage block-Jacobi GMRES(40) 1e-9; serve: Poisson stream of independent solves")
     ap.add_argument("--newton-tol", type=float, default=5e-13,
@@ -87,6 +88,13 @@ def parse():
 
 def workload(a) -> dict:
     prec = {"mixed": "FP32 blocks + FGMRES", "pc32": "FP64 Jacobian + FP32 ILU factors"}.get(a.precision, "FP64")
+    if a.workload == "batch":
+        return {"workload": f"batched linear solves: {a.systems} independent SDIRK3 Newton systems of the p={a.degree} "
+                            f"Euler vortex on periodic Voronoi meshes of 500-{a.max_seeds} cells (log-uniform, seeds "
+                            f"100+k), each at the 100k case's dt/h; GMRES(30) + block ILU(0) tol 1e-10, {prec}; one "
+                            f"step = all systems solved once",
+                "systems": a.systems, "degree": a.degree, "max_seeds": a.max_seeds, "precision": a.precision,
+                "l2": "small systems: the batch's matrices and factors (a few GB) stream once per iteration"}
     if a.workload == "serve":
         return {"workload": f"serving stream: {a.requests} independent solves, Poisson arrivals at {a.rate}/s; 50% "
                             f"advection (p in 1..3, random angle), 50% Euler vortex (p in 2..3, strength 1..5); "
@@ -253,9 +261,9 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    if a.workload == "serve":
-        print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop; its per-solve "
-                          "CPU cost is measured by the dirk3 and irk workloads"}), flush=True)
+    if a.workload in ("serve", "batch"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no serving loop or batched "
+                          "solver; its per-solve CPU cost is measured by the dirk3 and irk workloads"}), flush=True)
         return
     vals, info = [], None
     for k in range(a.warmup + a.steps):
@@ -451,6 +459,113 @@ def roofline(a, cp, ctx, eq, u, t, stream):
     return roof
 
 
+def run_batch(a):
+    """Solves/s of a set of independent Newton systems of uneven size: one
+    batched GMRES over the block-diagonal stack (segmented reductions, one
+    host synchronisation per restart cycle) against the same systems solved
+    one after another.  Inputs resident on the device; e2e copies the
+    right-hand sides in and the solutions out."""
+    import numpy as np
+    import torch
+
+    import cpolyg_b200 as cp
+
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    ctx = cp.Context(local)
+    rng = np.random.default_rng(7)
+    sizes = np.exp(rng.uniform(np.log(500), np.log(a.max_seeds), a.systems)).astype(int).tolist()
+    prec = cp.F32 if a.precision == "mixed" else cp.F64
+    flexible = a.precision == "mixed"
+    Js = []
+    for k, n in enumerate(sizes):
+        m = cp.PolyMesh.voronoi(cp.uniform_seeds(100 + k, n, WIDTH, WIDTH), WIDTH, WIDTH, periodic=True)
+        eq = cp.Euler(ctx, m, a.degree, gamma=GAMMA, dirichlet=(cp.INIT_VORTEX, VORTEX), exact_jacobian=True)
+        u = eq.interp(cp.INIT_VORTEX, VORTEX)
+        Js.append(eq.jacobian(u, 0.0, scale=-0.05 * (100000 / n) ** 0.5 * 0.435866521508459, add_mass=True,
+                              precision=prec))
+    Ps = [cp.BlockILU0(J, precision=prec) for J in Js]
+    S = cp.BlockMatrix.stack(Js)
+    PS = cp.BlockILU0(S, precision=prec)
+    gen = torch.Generator("cuda").manual_seed(1)
+    b = torch.randn(S.n_rows * S.bl, dtype=torch.float64, device="cuda", generator=gen)
+    seg = S.seg_rows
+    bl = S.bl
+    stream = torch.cuda.current_stream()
+
+    def one_by_one():
+        its = 0
+        for k, (J, P) in enumerate(zip(Js, Ps)):
+            bk = b[seg[k] * bl:seg[k + 1] * bl]
+            xk = torch.zeros_like(bk)
+            its += J.gmres(bk, xk, 30, 1e-10, 90000, P, flexible=flexible)[0]
+        return its
+
+    def batched():
+        x = torch.zeros_like(b)
+        return sum(i for i, _ in S.gmres_batched(seg, b, x, 30, 1e-10, 90000, PS, flexible=flexible)), x
+
+    for _ in range(a.warmup):
+        one_by_one()
+        batched()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = ctx.launches
+    e0.record(stream)
+    for _ in range(a.steps):
+        its_b, _ = batched()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1) / a.steps
+    launches = ctx.launches - launches0
+    e0.record(stream)
+    for _ in range(a.steps):
+        its_s = one_by_one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_s = e0.elapsed_time(e1) / a.steps
+    clk = clocks.stop()
+    # end to end: right-hand sides in from pinned host memory, solutions out
+    bh = b.cpu().pin_memory()
+    xh = torch.empty_like(bh).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        bd = bh.cuda(non_blocking=True)
+        x = torch.zeros_like(bd)
+        S.gmres_batched(seg, bd, x, 30, 1e-10, 90000, PS, flexible=flexible)
+        xh.copy_(x, non_blocking=True)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / a.steps
+    ms_max, value = replica_throughput(ms_b, a.systems, world, dist)
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32 blocks, f64 vectors" if flexible else "f64",
+               "data": "synthetic (seeded Voronoi meshes, analytic state)",
+               "config": dict(workload(a), parallelism=f"replicas x{world}", sizes=sizes),
+               "one_by_one": {"value": a.systems / (ms_s / 1e3), "unit": "solves/s", "ms_per_step": ms_s},
+               "gmres_iterations": {"batched": its_b, "one_by_one": its_s},
+               "e2e": {"value": a.systems / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(bh.numel() * 8),
+                       "d2h_bytes_per_step": int(xh.numel() * 8)},
+               "gpu_launches": launches, "clocks": clk}
+        print(json.dumps(out), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_ours(a):
     import numpy as np
     import torch
@@ -571,6 +686,8 @@ def main():
         run_reference(a)
     elif a.workload == "serve":
         run_serve(a)
+    elif a.workload == "batch":
+        run_batch(a)
     else:
         run_ours(a)
 

@@ -377,6 +377,31 @@ class BlockMatrix:
                                            C.byref(st)))
         return st.iterations, st.residual
 
+    @classmethod
+    def stack(cls, parts) -> "BlockMatrix":
+        """Block-diagonal stack of matrices of one block size and precision;
+        .seg_rows holds each part's first block row (and the total)."""
+        parts = list(parts)
+        ctx = parts[0].ctx
+        arr = (C.c_void_p * len(parts))(*[p.h.value if isinstance(p.h, C.c_void_p) else p.h for p in parts])
+        h = C.c_void_p()
+        ctx.check(ctx._lib.cpg_bsr_stack(ctx.h, len(parts), arr, C.byref(h)))
+        out = cls(ctx, h)
+        out.seg_rows = np.cumsum([0] + [p.n_rows for p in parts]).astype(np.int32)
+        return out
+
+    def gmres_batched(self, seg_rows, b, x, m: int, tol: float, maxIt: int, pc: "Preconditioner | None" = None,
+                      flexible: bool = False):
+        """Independent systems on the diagonal blocks [seg_rows[k],
+        seg_rows[k+1]) solved together; returns [(its, tol)] per system."""
+        seg = np.ascontiguousarray(seg_rows, dtype=np.int32)
+        K = len(seg) - 1
+        st = (_capi.SolveStats * K)()
+        self.ctx.check(self._lib.cpg_gmres_batched(self.ctx.h, self.h, pc.h if pc is not None else None, K, _pi(seg),
+                                                   C.c_void_p(_ptr(b)), C.c_void_p(_ptr(x)), m, tol, maxIt,
+                                                   int(flexible), st))
+        return [(s.iterations, s.residual) for s in st]
+
     def jacobi(self, b, x, tol: float, maxIt: int, pc: "BlockJacobi"):
         st = _capi.SolveStats()
         self.ctx.check(self._lib.cpg_jacobi_solve(self.ctx.h, self.h, pc.h, C.c_void_p(_ptr(b)),

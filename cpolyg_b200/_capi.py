@@ -83,6 +83,8 @@ PROTOTYPES = {
     "cpg_mesh_from_polygons": (I, [I, PI, PD, D, D, I, PI, PP]),
     "cpg_mesh_set_subtriangles": (I, [P, PI, PD]),
     "cpg_mesh_destroy": (None, [P]),
+    "cpg_gmres_batched": (I, [P, P, P, I, PI, P, P, I, D, I, I, C.POINTER(SolveStats)]),
+    "cpg_bsr_stack": (I, [P, I, PP, PP]),
     "cpg_mesh_write_gnuplot": (I, [P, C.c_char_p]),
     "cpg_field_write_gnuplot": (I, [P, P, P, P, C.c_char_p]),
     "cpg_bsr_write_spy": (I, [P, P, C.c_char_p]),

@@ -100,7 +100,8 @@ constexpr int MAX_ROW_BLOCKS = 64;
 template <class T, int BL, int VEC, int TPR>
 __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, const int *__restrict__ rowptr,
                                               const int *__restrict__ col, const T *__restrict__ vals,
-                                              const double *x, double *y, int mode) {
+                                              const double *x, double *y, int mode, const int *skip) {
+    if (skip && *skip) return;  // a Krylov solve that has converged
     static_assert((TPR * VEC) % BL == 0, "stride must be a multiple of the block size");
     static_assert(BL % VEC == 0, "vector width must divide the block size");
     constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
@@ -155,7 +156,9 @@ __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, cons
 template <class T>
 __global__ void __launch_bounds__(256) k_rows_dyn(int BL, int G, const int *__restrict__ rows,
                                                   const int *__restrict__ rowptr, const int *__restrict__ col,
-                                                  const T *__restrict__ vals, const double *x, double *y, int mode) {
+                                                  const T *__restrict__ vals, const double *x, double *y, int mode,
+                                                  const int *skip) {
+    if (skip && *skip) return;
     extern __shared__ double red_dyn[];
     __shared__ int scol[MAX_ROW_BLOCKS];
     const int i = rows ? rows[blockIdx.x] : blockIdx.x;
@@ -334,7 +337,8 @@ struct SweepSmem {
 template <class T, int BL>
 __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32)
     k_sweep(const int *__restrict__ order, int n, const int *__restrict__ rowptr, const int *__restrict__ col,
-            const T *__restrict__ vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
+            const T *__restrict__ vals, double *x, int mode, int *flags, int gen, int *counter, int *err, const int *skip) {
+    if (skip && *skip) return;  // a Krylov solve that has converged
     using Sh = SweepShape<T, BL>;
     using L = SweepSmem<T, BL>;
     constexpr int CT = Sh::CT, VEC = Sh::VEC, BPC = Sh::BPC, R = Sh::R;
@@ -539,7 +543,7 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
     k_sweep<T, BL><<<grid, threads, L::BYTES, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
-                                                            counter, err);
+                                                            counter, err, ctx->skip_dev);
     return launched(ctx, "sync-free sweep kernel");
 }
 
@@ -558,7 +562,8 @@ template <class T, int BL, int TPR>
 __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
     k_sweep_direct(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
                    const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags,
-                   int gen, int *counter, int *err) {
+                   int gen, int *counter, int *err, const int *skip) {
+    if (skip && *skip) return;  // a Krylov solve that has converged
     constexpr int VEC = SweepShape<T, BL>::VEC;
     constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
     constexpr int CLAIMER = TPR > 32 ? 32 : 0;  // warp 0 holds the dependency waits
@@ -650,7 +655,7 @@ cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, co
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
     k_sweep_direct<T, BL, TPR><<<grid, TPR, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags,
-                                                             gen, counter, err);
+                                                             gen, counter, err, ctx->skip_dev);
     return launched(ctx, "sync-free sweep kernel (direct)");
 }
 
@@ -700,19 +705,19 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
     // the widest variant because they are latency bound
 #define CPG_ROWS3(BLV, V, T0, T1, T2)                                                                    \
     switch (variant) {                                                                                   \
-        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;  \
-        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;  \
-        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break; \
+        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;  \
+        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;  \
+        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break; \
     }
     switch (bl) {
-        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;
-        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;
-        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode); break;
+        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;
+        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;
+        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;
         case 6: CPG_ROWS3(6, 2, 96, 192, 384) break;
         case 10: CPG_ROWS3(10, 2, 160, 320, 640) break;
         case 12:
-            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode);
-            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode);
+            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev);
+            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev);
             break;
         case 24:
             if constexpr (F32) { CPG_ROWS3(24, 4, 96, 192, 288) }
@@ -729,7 +734,8 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
         default: {
             if (bl > 256) return fail(ctx, CPG_ERR_UNSUPPORTED, "block size above 256");
             const int G = std::max(1, 256 / bl);
-            k_rows_dyn<T><<<nrows, 256, sizeof(double) * bl * G, s>>>(bl, G, rows, rowptr, col, vals, x, y, mode);
+            k_rows_dyn<T><<<nrows, 256, sizeof(double) * bl * G, s>>>(bl, G, rows, rowptr, col, vals, x, y, mode,
+                                                                     ctx->skip_dev);
         }
     }
 #undef CPG_ROWS3
@@ -953,6 +959,40 @@ cpg_status cpg_bsr_upload(cpg_ctx *ctx, cpg_bsr *A, const double *values_host) {
         cudaFree(tmp);
     }
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return CPG_OK;
+}
+
+cpg_status cpg_bsr_stack(cpg_ctx *ctx, int k, const cpg_bsr *const *parts, cpg_bsr **out) {
+    if (!ctx || k < 1 || !parts || !out) return CPG_ERR_INVALID_ARG;
+    *out = nullptr;
+    const int bl = parts[0]->bl, prec = parts[0]->precision;
+    std::vector<int> rowptr(1, 0), col;
+    int row0 = 0;
+    for (int q = 0; q < k; q++) {
+        const cpg_bsr *A = parts[q];
+        if (!A || A->bl != bl || A->precision != prec)
+            return fail(ctx, CPG_ERR_INVALID_ARG, "stacked matrices need one block size and precision");
+        for (int i = 0; i < A->n_rows; i++) {
+            for (int p = A->rowptr[i]; p < A->rowptr[i + 1]; p++) col.push_back(row0 + A->colidx[p]);
+            rowptr.push_back((int)col.size());
+        }
+        row0 += A->n_rows;
+    }
+    cpg_bsr *S = nullptr;
+    CPG_TRY(cpg_bsr_create_host(ctx, row0, bl, rowptr.data(), col.data(), nullptr, prec, &S));
+    const size_t b2 = (size_t)bl * bl * S->elem();
+    size_t at = 0;
+    for (int q = 0; q < k; q++) {
+        const size_t bytes = (size_t)parts[q]->nnzb * b2;
+        const cudaError_t e = cudaMemcpyAsync((char *)S->vals + at, parts[q]->vals, bytes, cudaMemcpyDeviceToDevice,
+                                              ctx->stream);
+        if (e != cudaSuccess) {
+            cpg_bsr_destroy(S);
+            return cuda_fail(ctx, e, "stacking matrix values");
+        }
+        at += bytes;
+    }
+    *out = S;
     return CPG_OK;
 }
 

@@ -26,6 +26,10 @@ struct cpg_ctx {
     // 1: cpg_precond_apply and cpg_assemble leave their device status words
     // to the next cpg_ctx_sync instead of synchronizing to read them
     int deferred_checks = 0;
+    // while a Krylov cycle is enqueued without host synchronisation: device
+    // word that is set once every system of the solve has converged; the
+    // block-row and sweep kernels then return at once (null otherwise)
+    const int *skip_dev = nullptr;
     // grow-only Krylov workspace (basis vectors), kept across solves
     double *kws = nullptr;
     size_t kws_cap = 0;  // doubles

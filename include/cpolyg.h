@@ -312,6 +312,11 @@ cpg_status cpg_bsr_get_info(const cpg_bsr *A, int *n_rows, int *bl,
 cpg_status cpg_bsr_export(cpg_ctx *ctx, const cpg_bsr *A, int *rowptr,
                           int *colidx, double *values_host);
 cpg_status cpg_bsr_upload(cpg_ctx *ctx, cpg_bsr *A, const double *values_host);
+/* k matrices of one block size and precision stacked block-diagonally into
+ * a new matrix (rows and columns of part q offset by the rows of the parts
+ * before it); for batched solves.  No counterpart in the reference.         */
+cpg_status cpg_bsr_stack(cpg_ctx *ctx, int k, const cpg_bsr *const *parts,
+                         cpg_bsr **out);
 
 /* Equation::jacobian (Equation.cpp:193-279) fused with
  * BlockMatrix::operator*= (BlockMatrix.cpp:297-308) and
@@ -385,6 +390,20 @@ typedef struct {
 cpg_status cpg_gmres(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P,
                      const double *b_dev, double *x_dev, int m, double tol,
                      int maxit, int flexible, cpg_solve_stats *stats);
+/* No counterpart in the reference (its GMRES solves one system).  nsys
+ * independent systems solved together: A is block diagonal, system k owning
+ * block rows [seg_rows[k], seg_rows[k+1]) (host array, nsys + 1 entries;
+ * cpg_bsr_stack builds such an A from separate matrices), P is A's
+ * preconditioner (for a block-diagonal A, ILU(0) and block Jacobi factor each
+ * system on its own), b and x stacked the same way.  Every system has its
+ * own Krylov basis coefficients, rotations and stopping test, with the same
+ * iterates as cpg_gmres on that system alone; one launch sequence serves all
+ * of them.  stats: nsys entries.  Rejects an A that couples two systems.    */
+cpg_status cpg_gmres_batched(cpg_ctx *ctx, const cpg_bsr *A,
+                             const cpg_precond *P, int nsys,
+                             const int *seg_rows_host, const double *b_dev,
+                             double *x_dev, int m, double tol, int maxit,
+                             int flexible, cpg_solve_stats *stats);
 /* damped block-Jacobi iteration, omega = 1 (BlockMatrix::jacobi)           */
 cpg_status cpg_jacobi_solve(cpg_ctx *ctx, const cpg_bsr *A,
                             const cpg_precond *P, const double *b_dev,
