@@ -4,8 +4,9 @@ one launch sequence, each with its own Krylov scalars and stopping test
 
 Each system's reductions run on the same fixed grid as a solve of that
 system alone, and its rows are computed row by row, so with the same
-triangular-sweep form the batched iterates equal the single solves' bit for
-bit: the same iteration counts and the same solutions."""
+triangular-sweep form and matvec variant the batched iterates equal the
+single solves' bit for bit: the same iteration counts and the same
+solutions."""
 import numpy as np
 import pytest
 import torch
@@ -32,8 +33,10 @@ def newton_matrices(ctx, sizes, degree=3, precision=cp.F64):
 
 @pytest.mark.parametrize("flexible,precision", [(False, cp.F64), (True, cp.F32)])
 def test_batched_gmres_equals_single_solves(ctx, monkeypatch, flexible, precision):
+    # the same triangular-sweep form alone and stacked, and every system
+    # large enough (>= 2048 block rows) for the tuned matvec variant
     monkeypatch.setenv("CPG_ILU_SWEEP", "form4")
-    sizes = [300, 700, 1500, 2600]
+    sizes = [2100, 2600, 3300, 4100]
     mats = newton_matrices(ctx, sizes, precision=precision)
     Js = [J for _, J in mats]
     gen = torch.Generator("cuda").manual_seed(3)
