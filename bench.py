@@ -64,7 +64,7 @@ def parse():
                     help="rebuild the Jacobian and preconditioner every k-th Newton iteration (0 = every one)")
     ap.add_argument("--newton-rtol", type=float, default=None,
                     help="also stop Newton only once the last update is below this, relative to the stage vector "
-                         "(default: 0, and 1e-9 for mixed, whose FP32-Jacobian Newton converges linearly)")
+                         "(default: 0, and 1e-8 for mixed, whose FP32-Jacobian Newton converges linearly)")
     ap.add_argument("--requests", type=int, default=512, help="serve: requests in the timed stream")
     ap.add_argument("--rate", type=float, default=200.0, help="serve: Poisson arrival rate, requests/s")
     ap.add_argument("--slots", type=int, default=8, help="serve: requests in flight at most")
@@ -73,7 +73,9 @@ def parse():
                     help="with --precision mixed: steps over which to measure the error against the FP64 path")
     a = ap.parse_args()
     if a.newton_rtol is None:
-        a.newton_rtol = 1e-9 if a.precision == "mixed" else 0.0
+        # the FP32-Jacobian Newton converges linearly; 1e-8 on the update keeps
+        # the 20-step result within 1e-8 of the FP64 path (5.2e-9 measured)
+        a.newton_rtol = 1e-8 if a.precision == "mixed" else 0.0
     if a.workload == "irk":
         if a.cells == 100000:
             a.cells = 500000

@@ -60,3 +60,40 @@ def test_admission_respects_the_memory_budget():
     stats = srv.serve(reqs, realtime=False)
     assert stats["failed"] == 0
     assert srv.peak_bytes <= biggest
+
+
+@pytest.mark.gpu
+def test_served_results_match_the_oracle():
+    """A sample of served requests, each against the oracle run of the same
+    problem (same seeded mesh, physics, stepper, time step and steps):
+    relative 2-norm difference <= 1e-11 (FP64)."""
+    import cpolyg_b200 as cp
+    import oracle
+    reqs = serve.make_stream(8, rate=400.0, seed=11, min_seeds=200, max_seeds=600, min_steps=2, max_steps=4)
+    srv = serve.Server(slots=4)
+    stats = srv.serve(reqs, realtime=True)
+    assert stats["failed"] == 0
+    kinds = set()
+    for r in reqs:
+        L = serve.domain(r)
+        m = cp.PolyMesh.voronoi(cp.uniform_seeds(r.seed, r.n_seeds, L, L), L, L, periodic=True)
+        om = oracle.Mesh(m.export())
+        if r.physics == "advection":
+            oe = oracle.Equation(om, 0, r.degree, beta=(math.cos(r.angle), math.sin(r.angle)))
+            u = oe.interp(cp.INIT_GAUSSIAN, [100.0, 0.5, 0.5])
+        else:
+            vort = [r.strength, 5.0, 5.0, 1.0, 1.0, 1.4, 10.0, 10.0]
+            oe = oracle.Equation(om, 2, r.degree, dkind=cp.INIT_VORTEX, dparams=vort, exact_jacobian=True)
+            u = oe.interp(cp.INIT_VORTEX, vort)
+        if r.stepper == "rk4":
+            st = oracle.Stepper(oe, cp.STEP_RK4)
+        else:
+            st = oracle.Stepper(oe, cp.STEP_SDIRK3, pc=2, gmres_m=30, gmres_tol=1e-10, gmres_maxit=90000)
+        t = 0.0
+        for _ in range(r.steps):
+            u = st.advance(u, r.dt, t)
+            t += r.dt
+        err = np.linalg.norm(r.result - u) / np.linalg.norm(u)
+        assert err < 1e-11, (r.rid, r.physics, r.stepper, err)
+        kinds.add((r.physics, r.stepper))
+    assert len(kinds) >= 3  # the sample covers the mix
