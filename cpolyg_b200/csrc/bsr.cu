@@ -14,6 +14,7 @@
 // with rows streamed straight into registers, or k_sweep with a TMA ring), or
 // one launch per level of the level schedule computed from the block pattern.
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -525,20 +526,13 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
                             const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
     using L = SweepSmem<T, BL>;
     constexpr int threads = SweepShape<T, BL>::CT + 32;
-    // set once per device and instantiation (repeating it is harmless)
-    static bool attr_set[64] = {};
-    static int per_sm[64] = {};
-    const bool known = ctx->device >= 0 && ctx->device < 64 && attr_set[ctx->device];
-    int occ = known ? per_sm[ctx->device] : 0;
-    if (!known) {
-        if (L::BYTES > 48 * 1024)
-            CPG_CUDA(ctx, cudaFuncSetAttribute(k_sweep<T, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)L::BYTES));
+    static std::atomic<int> per_sm[64];  // occupancy per device, computed once
+    CPG_TRY(smem_limit_once(ctx, (const void *)k_sweep<T, BL>, (int)L::BYTES));
+    const bool cacheable = ctx->device >= 0 && ctx->device < 64;
+    int occ = cacheable ? per_sm[ctx->device].load() : 0;
+    if (!occ) {
         CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep<T, BL>, threads, L::BYTES));
-        if (ctx->device >= 0 && ctx->device < 64) {
-            per_sm[ctx->device] = occ;
-            attr_set[ctx->device] = true;
-        }
+        if (cacheable) per_sm[ctx->device].store(occ);
     }
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
@@ -645,12 +639,12 @@ template <class T, int BL, int TPR>
 cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
                                    const T *vals, double *x, int mode, int *flags, int gen, int *counter,
                                    int *err) {
-    static int per_sm[64] = {};
+    static std::atomic<int> per_sm[64];  // occupancy per device, computed once
     const bool cacheable = ctx->device >= 0 && ctx->device < 64;
-    int occ = cacheable ? per_sm[ctx->device] : 0;
+    int occ = cacheable ? per_sm[ctx->device].load() : 0;
     if (!occ) {
         CPG_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_sweep_direct<T, BL, TPR>, TPR, 0));
-        if (cacheable) per_sm[ctx->device] = occ;
+        if (cacheable) per_sm[ctx->device].store(occ);
     }
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));

@@ -44,6 +44,14 @@ cpg_status scratch(cpg_ctx *ctx, size_t n, double **out);
 cpg_status pinned(cpg_ctx *ctx, size_t n, double **out);
 // check the last launch; increments the launch counter
 cpg_status launched(cpg_ctx *ctx, const char *what);
+// Raises a kernel's dynamic shared-memory limit to `bytes` (or leaves it if
+// already raised) on the context's device, once: the first call for a
+// (kernel, device) sets it and records it under a process-wide lock, later
+// calls only look it up.  Callers pass the largest size the kernel is ever
+// launched with.  The driver does not tolerate the attribute being set while
+// another host thread launches the same kernel (one context per thread in
+// the serving loop), so no launch site may set it directly.
+cpg_status smem_limit_once(cpg_ctx *ctx, const void *kernel, int bytes);
 // slot of ctx->flag_dev where the residual kernel records the first cell
 // (+1) whose state is not admissible (0 = none)
 constexpr int FLAG_NONPHYS = 8;

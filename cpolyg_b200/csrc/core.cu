@@ -2,7 +2,10 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <utility>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -61,6 +64,21 @@ cpg_status launched(cpg_ctx *ctx, const char *what) {
     ctx->launches++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(ctx, e, what);
+    return CPG_OK;
+}
+
+cpg_status smem_limit_once(cpg_ctx *ctx, const void *kernel, int bytes) {
+    if (bytes <= 48 * 1024) return CPG_OK;
+    static std::mutex mu;
+    static std::map<std::pair<const void *, int>, int> done;
+    std::lock_guard<std::mutex> lk(mu);
+    int &have = done[{kernel, ctx->device}];
+    if (have >= bytes) return CPG_OK;
+    if (have > 0)  // a second, larger value would race with launches in flight
+        return fail(ctx, CPG_ERR_UNSUPPORTED, "kernel shared-memory limit raised twice");
+    const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaFuncSetAttribute(MaxDynamicSharedMemorySize)");
+    have = bytes;
     return CPG_OK;
 }
 

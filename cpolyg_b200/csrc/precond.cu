@@ -752,7 +752,7 @@ cpg_status launch_factor_tc(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     // dynamic shared memory of at least 57 KB keeps at most 4 CTAs (4 x 128
     // TMEM columns) on an SM, so no TMEM allocation ever waits for another CTA
     const size_t smem = std::max<size_t>(tcf::smem_bytes(SPLIT), 57 * 1024);
-    CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor_tc<SPLIT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CPG_TRY(smem_limit_once(ctx, (const void *)k_ilu_factor_tc<SPLIT>, (int)smem));
     k_ilu_factor_tc<SPLIT><<<nrows, tcf::NT, smem, ctx->stream>>>(
         rows, (const float *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
         P->lp_u_d, (float *)P->L_vals, (float *)P->U_vals, P->dinv64, P->dinv_idx_d, ctx->flag_dev);
@@ -763,9 +763,7 @@ cpg_status launch_factor_tc(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     const size_t per_warp = (b2 + 8 * (size_t)(BL - 8) + BL) * sizeof(double);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
     const size_t ismem = per_warp * wpb;
-    if ((int)ismem > 48 * 1024)
-        CPG_CUDA(ctx, cudaFuncSetAttribute(k_block_inverse<float, 40>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)ismem));
+    CPG_TRY(smem_limit_once(ctx, (const void *)k_block_inverse<float, 40>, (int)ismem));
     k_block_inverse<float, 40><<<(nrows + wpb - 1) / wpb, 32 * wpb, ismem, ctx->stream>>>(
         BL, nrows, rows, (float *)P->U_vals, P->U_rowptr_d, P->dinv64, P->dinv_idx_d, ctx->flag_dev);
     return launched(ctx, "pivot block inverse kernel");
@@ -781,9 +779,11 @@ cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     const int BL = P->bl;
     const int ld = (BLC > 0 && BLC % 8 == 0) ? BL + 4 : BL;  // padded blocks on the DMMA path
     const size_t smem = 5 * (size_t)BL * ld * sizeof(double) + 16;
-    if ((int)smem > 48 * 1024)  // per launch: contexts on several host threads may share the kernel
-        CPG_CUDA(ctx, cudaFuncSetAttribute(k_ilu_factor<TA, TS, BLC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)smem));
+    // compiled-in block sizes have one size; the generic kernel gets the
+    // whole shared memory of a CTA, so its limit is raised once for any size
+    CPG_TRY(smem_limit_once(ctx, (const void *)k_ilu_factor<TA, TS, BLC>,
+                            BLC > 0 ? (int)smem : (smem > 48 * 1024 ? 227 * 1024 : 0)));
+    if (smem > 227 * 1024) return fail(ctx, CPG_ERR_UNSUPPORTED, "block too large for the factor kernel");
     double *dinv = P->precision == CPG_F64 ? (double *)P->U_vals : P->dinv64;
     k_ilu_factor<TA, TS, BLC><<<nrows, FT, smem, ctx->stream>>>(
         BL, rows, (const TA *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
@@ -796,9 +796,8 @@ cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
     const size_t ismem = per_warp * wpb;
     if (ismem > 227 * 1024) return fail(ctx, CPG_ERR_UNSUPPORTED, "pivot block too large for shared memory");
-    if ((int)ismem > 48 * 1024)
-        CPG_CUDA(ctx, cudaFuncSetAttribute(k_block_inverse<TS, BLC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)ismem));
+    CPG_TRY(smem_limit_once(ctx, (const void *)k_block_inverse<TS, BLC>,
+                            BLC > 0 ? (int)ismem : (ismem > 48 * 1024 ? 227 * 1024 : 0)));
     k_block_inverse<TS, BLC><<<(nrows + wpb - 1) / wpb, 32 * wpb, ismem, ctx->stream>>>(
         BL, nrows, rows, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
     return launched(ctx, "pivot block inverse kernel");
