@@ -3,7 +3,8 @@
 * ``oracle/_build/liboracle.so`` from ``oracle/oracle.cpp`` (the CPU
   restatement of the reference, OpenMP over cells), always.
 * ``oracle/_ref/`` from the reference's own sources, only when they are
-  present (``/root/reference``): the vendored Triangle and Voro++ 2D
+  present (``CPOLYG_REFERENCE_SRC``, by default ``/root/reference``): the
+  vendored Triangle and Voro++ 2D
   libraries, compiled unmodified where they lie, plus the small driver
   ``oracle/ref_mesh_driver.cpp`` that calls them the way
   ``PolyMesh(pts, w, h)`` and ``Triangulation`` do (src/PolyMesh.cpp:162-218,
@@ -20,7 +21,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 BUILD = os.path.join(HERE, "_build")
 REF_OUT = os.path.join(HERE, "_ref")
-REF_SRC = "/root/reference"
+# the reference's source tree (read only); CPOLYG_REFERENCE_SRC overrides it
+REF_SRC = os.environ.get("CPOLYG_REFERENCE_SRC", "/root/reference")
 
 CXXFLAGS = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-fPIC", "-std=c++17"]
 

@@ -28,13 +28,25 @@ def test_noalloc_norm_matches_allocating_norm_on_two_calls(ctx, name, deg):
     ge, oe, _ = equations(ctx, name, deg, n=300, periodic=True)
     kind, params = (cp.INIT_VORTEX, [5.0, 0.5, 0.5, 1, 1, 1.4, 1, 1]) if name == "euler" else \
         (cp.INIT_GAUSSIAN, [30.0, 0.4, 0.6])
+    import torch
     u1 = ge.interp(kind, params)
     u2 = u1 * -3.0 + 0.25
+    refs = [ge.L2Norm(u) for u in (u1, u2)]  # the allocating entry point, first
     lib = cp.lib()
-    for u in (u1, u2):
-        out = np.zeros(4)
+    outs = [np.zeros(4) for _ in range(3)]
+
+    def call(u, out):
         st = lib.cpg_l2norm_noalloc(ctx.h, ge.h, C.c_void_p(u.data_ptr()), out.ctypes.data_as(C.POINTER(C.c_double)))
         assert st == 0, lib.cpg_last_error(ctx.h)
-        ref = ge.L2Norm(u)
+
+    call(u1, outs[2])  # set-up call: looks up the static array's device address
+    torch.cuda.synchronize()
+    alloc0, free0 = torch.cuda.memory_allocated(), torch.cuda.mem_get_info()[0]
+    for u, out in zip((u1, u2), outs):
+        call(u, out)
+    torch.cuda.synchronize()
+    # the two calls allocated nothing, through torch or the driver
+    assert torch.cuda.memory_allocated() == alloc0 and torch.cuda.mem_get_info()[0] == free0
+    for out, ref in zip(outs, refs):
         got = out[: ge.nc]
         assert np.all(np.abs(got - ref) <= TOL * np.abs(ref).max())
