@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
 // ---------------------------------------------------------------------------
 template <int NB>
 __global__ void k_mass(int n, int nc, const double *__restrict__ Mi, const double *__restrict__ x, double alpha,
-                       const double *__restrict__ z, double beta, double *__restrict__ y) {
+                       const double *__restrict__ z, double beta, double *__restrict__ y, const int *skip) {
+    if (skip && *skip) return;  // a Krylov solve that has converged
     const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int BL = NB * nc;
     if (idx >= (int64_t)n * BL) return;
@@ -848,9 +849,9 @@ static cpg_status mass_op(cpg_ctx *ctx, const cpg_equation *eq, const double *Mi
     const int T = 256;
     const int grid = (int)((N + T - 1) / T);
     switch (eq->nb) {
-        case 3: k_mass<3><<<grid, T, 0, ctx->stream>>>(eq->n, eq->nc, Mi, x, alpha, z, beta, y); break;
-        case 6: k_mass<6><<<grid, T, 0, ctx->stream>>>(eq->n, eq->nc, Mi, x, alpha, z, beta, y); break;
-        case 10: k_mass<10><<<grid, T, 0, ctx->stream>>>(eq->n, eq->nc, Mi, x, alpha, z, beta, y); break;
+        case 3: k_mass<3><<<grid, T, 0, ctx->stream>>>(eq->n, eq->nc, Mi, x, alpha, z, beta, y, ctx->skip_dev); break;
+        case 6: k_mass<6><<<grid, T, 0, ctx->stream>>>(eq->n, eq->nc, Mi, x, alpha, z, beta, y, ctx->skip_dev); break;
+        case 10: k_mass<10><<<grid, T, 0, ctx->stream>>>(eq->n, eq->nc, Mi, x, alpha, z, beta, y, ctx->skip_dev); break;
         default: return fail(ctx, CPG_ERR_UNSUPPORTED, "basis size");
     }
     return launched(ctx, "mass kernel");

@@ -81,7 +81,8 @@ __global__ void k_axpby(int64_t N, double a, const double *__restrict__ x, doubl
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x)
         y[q] = a * x[q] + b * y[q];
 }
-__global__ void k_copy(int64_t N, const double *__restrict__ x, double *__restrict__ y) {
+__global__ void k_copy(int64_t N, const double *__restrict__ x, double *__restrict__ y, const int *skip) {
+    if (skip && *skip) return;  // a Krylov solve that has converged
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x)
         y[q] = x[q];
 }
@@ -145,7 +146,7 @@ cpg_status vec_axpby(cpg_ctx *ctx, int64_t n, double a, const double *x, double 
 }
 cpg_status vec_copy(cpg_ctx *ctx, int64_t n, const double *x, double *y) {
     if (n <= 0) return CPG_OK;
-    k_copy<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, x, y);
+    k_copy<<<grid_for(ctx, n), 256, 0, ctx->stream>>>(n, x, y, ctx->skip_dev);
     return launched(ctx, "copy kernel");
 }
 cpg_status vec_fill(cpg_ctx *ctx, int64_t n, double v, double *y) {
@@ -417,9 +418,9 @@ cpg_status gmres_seg_run(cpg_ctx *ctx, const LinOp &op, int K, const int64_t *of
     const int HS = m + 4, HP = m * (m + 1) / 2 + 1;
     const size_t n_part = (size_t)CPS * K * (m + 2);
     const size_t n_dbl = n_part + (size_t)K * (HS + HP + 2 * m + 2 * (m + 1) + 2);
-    const size_t n_int = (size_t)6 * K + 2;  // off (int64, 2 ints each) counted separately below
+    // after the doubles: K + 1 int64 offsets, then 4K + 2 ints
     double *sc;
-    CPG_TRY(scratch(ctx, n_dbl + (size_t)(K + 1) + n_int / 2 + 4, &sc));
+    CPG_TRY(scratch(ctx, n_dbl + (size_t)(K + 1) + (size_t)(2 * K + 1) + 4, &sc));
     double *part = sc;
     KState st;
     st.m = m;
@@ -451,7 +452,6 @@ cpg_status gmres_seg_run(cpg_ctx *ctx, const LinOp &op, int K, const int64_t *of
     CPG_TRY(seg_norm(ctx, sg, r, part, st.nrm2b, 2, 0, nullptr));
     if (maxit % m > 0) maxit = (maxit / m + 1) * m;
     const int cycles = maxit / m;
-    std::vector<int> fin(K, 0), hst(2);
     int j;
     cpg_status rc = CPG_OK;
     for (j = 0; j < cycles && rc == CPG_OK; j++) {
@@ -514,8 +514,9 @@ cpg_status gmres_seg_run(cpg_ctx *ctx, const LinOp &op, int K, const int64_t *of
         k_seg_combine<<<vgrid, 256, 0, ctx->stream>>>(sg, N, flexible ? Z : V, st.cy, m + 1, st.nsteps, x);
         CPG_TRY(launched(ctx, "solution update kernel"));
         // one read-back per cycle: which systems have converged, and status
-        int *hp;
-        CPG_TRY(pinned(ctx, (K + 2) / 2 + 1, (double **)&hp));
+        double *hbuf;
+        CPG_TRY(pinned(ctx, (size_t)(K + 2) / 2 + 1, &hbuf));
+        int *hp = reinterpret_cast<int *>(hbuf);  // K + 1 ints
         CPG_CUDA(ctx, cudaMemcpyAsync(hp, st.finished, sizeof(int) * K, cudaMemcpyDeviceToHost, ctx->stream));
         CPG_CUDA(ctx, cudaMemcpyAsync(hp + K, st.status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
         CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

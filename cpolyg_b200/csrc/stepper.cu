@@ -22,7 +22,10 @@ struct Comb {
     double a[8];
     int nk;
 };
-__global__ void k_combine(int64_t N, const double *__restrict__ u, Comb c, double *__restrict__ out) {
+// skip: a Krylov solve's converged word (null outside a solve's cycle)
+__global__ void k_combine(int64_t N, const double *__restrict__ u, Comb c, double *__restrict__ out,
+                          const int *skip) {
+    if (skip && *skip) return;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x) {
         double v = u ? u[q] : 0.0;
         for (int j = 0; j < c.nk; j++) v = v + c.a[j] * c.k[j][q];
@@ -90,7 +93,8 @@ __global__ void k_build_stage_blocks(int n, int s, int nb, int nc, const T *__re
 }
 // stage-major [stage][cell][bl] <-> cell-major [cell][stage][bl]
 __global__ void k_stage_perm(int n, int s, int bl, const double *__restrict__ in, double *__restrict__ out,
-                             int to_cell) {
+                             int to_cell, const int *skip) {
+    if (skip && *skip) return;
     const int64_t N = (int64_t)n * s * bl;
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < N; q += (int64_t)gridDim.x * blockDim.x) {
         // q indexes the stage-major vector
@@ -320,7 +324,7 @@ struct StageOp : LinOp {
                 cb.k[j] = x + j * N;
                 cb.a[j] = S->A[i * s + j];
             }
-            k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, nullptr, cb, S->tmp);
+            k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, nullptr, cb, S->tmp, ctx->skip_dev);
             CPG_TRY(launched(ctx, "stage combine kernel"));
             CPG_TRY(bsr_matvec_raw(ctx, S->Jview[i], S->tmp, S->dk));
             CPG_TRY(mass_apply_axpy(ctx, S->eq, x + i * N, 1.0, S->dk, -dt, y + i * N));
@@ -330,10 +334,10 @@ struct StageOp : LinOp {
     cpg_status prec(cpg_ctx *ctx, double *x) const override {
         const int n = S->eq->n, s = S->s, bl = S->eq->bl;
         const int64_t NS = S->N * s;
-        k_stage_perm<<<grid_for(ctx, NS), 256, 0, ctx->stream>>>(n, s, bl, x, S->big2, 1);
+        k_stage_perm<<<grid_for(ctx, NS), 256, 0, ctx->stream>>>(n, s, bl, x, S->big2, 1, ctx->skip_dev);
         CPG_TRY(launched(ctx, "stage permute kernel"));
         CPG_TRY(precond_apply_raw(ctx, S->P, S->big2));
-        k_stage_perm<<<grid_for(ctx, NS), 256, 0, ctx->stream>>>(n, s, bl, S->big2, x, 0);
+        k_stage_perm<<<grid_for(ctx, NS), 256, 0, ctx->stream>>>(n, s, bl, S->big2, x, 0, ctx->skip_dev);
         return launched(ctx, "stage permute kernel");
     }
 };
@@ -365,7 +369,7 @@ cpg_status combine(cpg_stepper *S, const double *u, std::initializer_list<std::p
         cb.a[cb.nk] = t.second;
         cb.nk++;
     }
-    k_combine<<<grid_for(S->ctx, S->N), 256, 0, S->ctx->stream>>>(S->N, u, cb, out);
+    k_combine<<<grid_for(S->ctx, S->N), 256, 0, S->ctx->stream>>>(S->N, u, cb, out, S->ctx->skip_dev);
     return launched(S->ctx, "combine kernel");
 }
 
@@ -465,7 +469,7 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
                 cb.k[j] = S->k + j * N;
                 cb.a[j] = S->A[stage * s + j];
             }
-            k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu);
+            k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu, ctx->skip_dev);
             CPG_TRY(launched(ctx, "stage combine kernel"));
             CPG_TRY(assemble_raw(ctx, S->eq, S->cu, ts, S->rhs));
             CPG_TRY(mass_apply_axpy(ctx, S->eq, ks, 1.0, S->rhs, -dt, S->r));  // r = M k - dt rhs
@@ -511,7 +515,7 @@ cpg_status dirk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_st
         cb.k[i] = S->k + i * N;
         cb.a[i] = S->b[i];
     }
-    k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, u);
+    k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, u, ctx->skip_dev);
     return launched(ctx, "stage combine kernel");
 }
 
@@ -541,7 +545,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                     cb.k[j] = K + j * N;
                     cb.a[j] = S->Ainv[i * s + j];
                 }
-                k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, nullptr, cb, S->tmp);
+                k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, nullptr, cb, S->tmp, ctx->skip_dev);
                 CPG_TRY(launched(ctx, "stage combine kernel"));
                 CPG_TRY(combine(S, u, {{K + i * N, 1.0}}, S->cu));  // u + w_i
                 CPG_TRY(assemble_raw(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
@@ -561,7 +565,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                     cb.k[j] = K + j * N;
                     cb.a[j] = S->A[i * s + j];
                 }
-                k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu);
+                k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu, ctx->skip_dev);
                 CPG_TRY(launched(ctx, "stage combine kernel"));
                 CPG_TRY(assemble_raw(ctx, S->eq, S->cu, t + dt * S->c[i], S->rhs));
                 CPG_TRY(mass_apply_axpy(ctx, S->eq, K + i * N, 1.0, S->rhs, -dt, R + i * N));
@@ -591,7 +595,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                     cb.k[j] = K + j * N;
                     cb.a[j] = S->A[i * s + j];
                 }
-                k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu);
+                k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, S->cu, ctx->skip_dev);
                 CPG_TRY(launched(ctx, "stage combine kernel"));
             }
             CPG_TRY(cpg_jacobian(ctx, S->eq, S->cu, t + dt * S->c[i], 1.0, 0, S->Jview[i]));
@@ -659,7 +663,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
             cb.a[i] = S->b[i];
         }
     }
-    k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, u);
+    k_combine<<<grid_for(ctx, N), 256, 0, ctx->stream>>>(N, u, cb, u, ctx->skip_dev);
     return launched(ctx, "stage combine kernel");
 }
 
