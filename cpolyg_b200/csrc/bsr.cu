@@ -98,10 +98,29 @@ struct SmemLoad<float, 4> {
 
 constexpr int MAX_ROW_BLOCKS = 64;
 
+constexpr int PREFETCH_ROWS = 50000;  // below this many rows a launch is latency-bound
+
+// Bulk prefetch of a row's blocks into L2 (cp.async.bulk.prefetch.L2, no
+// multicast), one block per lane of the calling warp: issued as soon as the
+// row is known, so that the streaming loads that follow hit L2.  Only for
+// block sizes whose blocks are whole multiples of 16 bytes (the bulk copy's
+// granule); the row starts 16-byte aligned then too.
+template <class T, int BL>
+__device__ __forceinline__ void prefetch_row_l2(const T *vals, int k0, int nblk, int lane) {
+    constexpr unsigned B = BL * BL * sizeof(T);
+    if constexpr (B % 16 == 0) {
+        for (int b = lane; b < nblk; b += 32)
+            asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(vals + (size_t)(k0 + b) * BL * BL),
+                         "r"(B)
+                         : "memory");
+    }
+}
+
 template <class T, int BL, int VEC, int TPR>
 __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, const int *__restrict__ rowptr,
                                               const int *__restrict__ col, const T *__restrict__ vals,
-                                              const double *x, double *y, int mode, const int *skip) {
+                                              const double *x, double *y, int mode, const int *skip,
+                                              int prefetch) {
     if (skip && *skip) return;  // a Krylov solve that has converged
     static_assert((TPR * VEC) % BL == 0, "stride must be a multiple of the block size");
     static_assert(BL % VEC == 0, "vector width must divide the block size");
@@ -111,6 +130,7 @@ __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, cons
     const int i = rows ? rows[blockIdx.x] : blockIdx.x;
     const int k0 = rowptr[i], nblk = rowptr[i + 1] - k0;
     const int tid = threadIdx.x;
+    if (prefetch && tid < 32) prefetch_row_l2<T, BL>(vals, k0, nblk, tid);
     for (int q = tid; q < nblk && q < MAX_ROW_BLOCKS; q += TPR) scol[q] = col[k0 + q];
     __syncthreads();
     const int e0 = tid * VEC;
@@ -556,7 +576,7 @@ template <class T, int BL, int TPR>
 __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
     k_sweep_direct(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
                    const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags,
-                   int gen, int *counter, int *err, const int *skip) {
+                   int gen, int *counter, int *err, const int *skip, int prefetch) {
     if (skip && *skip) return;  // a Krylov solve that has converged
     constexpr int VEC = SweepShape<T, BL>::VEC;
     constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
@@ -575,11 +595,16 @@ __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
     for (int cur = 0;; cur ^= 1) {
         const int q = s_row[cur];
         if (q >= n) break;
-        if (tid == CLAIMER) s_row[cur ^ 1] = atomicAdd(counter, 1);  // in flight while this row streams
+        // the next claim stays in flight while this row streams: its result
+        // is stored to shared memory only after the streaming loop
+        const int next = tid == CLAIMER ? atomicAdd(counter, 1) : 0;
         const int i = order[q];
         const int k0 = rowptr[i], nraw = rowptr[i + 1] - k0;
         const int nblk = nraw > SWEEP_MAXB ? 0 : nraw;  // the host admits no longer rows
         if (tid == 0 && nraw > SWEEP_MAXB) atomicExch(err, 3);
+        // the row's values do not depend on the rows it waits for: on a
+        // latency-bound sweep (few rows) they are fetched into L2 meanwhile
+        if (prefetch && tid >= TPR - 32) prefetch_row_l2<T, BL>(vals, k0, nblk, tid - (TPR - 32));
         for (int b = tid; b < nblk; b += TPR) {
             const int j = col[k0 + b];
             scol[b] = j;
@@ -616,6 +641,7 @@ __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
                 blk++;
             }
         }
+        if (tid == CLAIMER) s_row[cur ^ 1] = next;
 #pragma unroll
         for (int v = 0; v < VEC; v++) red[g][r0 + v] = acc[v];
         __syncthreads();
@@ -649,7 +675,8 @@ cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, co
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
     k_sweep_direct<T, BL, TPR><<<grid, TPR, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags,
-                                                             gen, counter, err, ctx->skip_dev);
+                                                             gen, counter, err, ctx->skip_dev,
+                                                             nrows < PREFETCH_ROWS ? 1 : 0);
     return launched(ctx, "sync-free sweep kernel (direct)");
 }
 
@@ -694,24 +721,28 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
     if (nrows <= 0) return CPG_OK;
     cudaStream_t s = ctx->stream;
     constexpr bool F32 = std::is_same<T, float>::value;
+    // L2 prefetch of each row where rows are latency-bound: FP32 values
+    // (half the bytes per row for the same per-row work) and launches of few
+    // rows; a full FP64 matvec streams at the copy bandwidth without it
+    const int pf = (F32 || nrows < PREFETCH_ROWS) ? 1 : 0;
     // threads per row: variants 0/1/2 use about 8/16/32 column groups; the
     // matvec picks its variant by timing (autotune below), level sweeps take
     // the widest variant because they are latency bound
 #define CPG_ROWS3(BLV, V, T0, T1, T2)                                                                    \
     switch (variant) {                                                                                   \
-        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;  \
-        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;  \
-        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break; \
+        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;  \
+        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;  \
+        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break; \
     }
     switch (bl) {
-        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;
-        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;
-        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev); break;
+        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;
+        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;
+        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;
         case 6: CPG_ROWS3(6, 2, 96, 192, 384) break;
         case 10: CPG_ROWS3(10, 2, 160, 320, 640) break;
         case 12:
-            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev);
-            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev);
+            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf);
+            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf);
             break;
         case 24:
             if constexpr (F32) { CPG_ROWS3(24, 4, 96, 192, 288) }
