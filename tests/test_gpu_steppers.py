@@ -251,3 +251,27 @@ def test_nonphysical_state_is_reported_by_name(ctx):
     with pytest.raises(cp.CpgError) as e:
         step.advance(u, 0.05, 0.0)
     assert e.value.status == 10 and f"cell {bad}" in str(e.value) and "Newton iteration 0" in str(e.value)
+
+
+def test_deferred_checks_report_at_sync(ctx):
+    """With deferred checks the residual of a non-physical state returns at
+    once and the next cpg_ctx_sync reports it (cell named); afterwards the
+    word is clear and checks are immediate again."""
+    import torch
+    ge, oe, _ = equations(ctx, "euler", 2, n=200, periodic=True, width=10.0)
+    u0 = oe.interp(*VORTEX).reshape(ge.np, ge.nc, ge.nb)
+    u0[11, 3, 0] = -1.0
+    u = to_dev(u0).reshape(ge.np, ge.nc, ge.nb)
+    b = torch.empty_like(u)
+    lib = ctx._lib
+    ctx.check(lib.cpg_ctx_set_deferred_checks(ctx.h, 1))
+    try:
+        assert lib.cpg_assemble(ctx.h, ge.h, cp.C.c_void_p(u.data_ptr()), 0.0, cp.C.c_void_p(b.data_ptr())) == 0
+        with pytest.raises(cp.CpgError) as e:
+            ctx.sync()
+        assert e.value.status == 10 and "cell 11" in str(e.value)
+        ctx.sync()  # cleared
+    finally:
+        ctx.check(lib.cpg_ctx_set_deferred_checks(ctx.h, 0))
+    st = lib.cpg_assemble(ctx.h, ge.h, cp.C.c_void_p(u.data_ptr()), 0.0, cp.C.c_void_p(b.data_ptr()))
+    assert st == 10
