@@ -232,12 +232,26 @@ __global__ void __launch_bounds__(RT) k_seg_cgs(Seg sg, int64_t N, int nv, const
     for (int l = threadIdx.x; l < nv; l += RT) sh_h[l] = -h[(size_t)seg * stride + l];
     __syncthreads();
     const int64_t a = sg.off[seg], b = sg.off[seg + 1];
+    constexpr int64_t STRIDE = (int64_t)CPS * RT;
     double s = 0.0;
-    for (int64_t q = a + (int64_t)blockIdx.x * RT + threadIdx.x; q < b; q += (int64_t)CPS * RT) {
-        double x = w[q];
-        for (int l = 0; l < nv; l++) x += sh_h[l] * V[(size_t)l * N + q];
+    // two elements of the thread's sequence at a time (two independent
+    // chains of loads in flight); each element, and the order in which the
+    // thread sums their squares, is as for one element at a time
+    for (int64_t q = a + (int64_t)blockIdx.x * RT + threadIdx.x; q < b; q += 2 * STRIDE) {
+        const int64_t q2 = q + STRIDE;
+        const bool two = q2 < b;
+        double x = w[q], x2 = two ? w[q2] : 0.0;
+        for (int l = 0; l < nv; l++) {
+            const double hl = sh_h[l];
+            x += hl * V[(size_t)l * N + q];
+            if (two) x2 += hl * V[(size_t)l * N + q2];
+        }
         w[q] = x;
         s += x * x;
+        if (two) {
+            w[q2] = x2;
+            s += x2 * x2;
+        }
     }
     s = block_sum(s, sh);
     if (threadIdx.x == 0) part[(size_t)seg * CPS + blockIdx.x] = s;
