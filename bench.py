@@ -419,6 +419,7 @@ def roofline(a, cp, ctx, eq, u, t, stream):
     s_a = 4 if mixed else 8
     s_p = 4 if a.precision in ("mixed", "pc32") else 8
     gamma = 0.435866521508459 if a.tableau == "sdirk3" else 0.717933260754229
+    gmres_tol = 1e-10  # the stepper's
     J = eq.jacobian(u, t, scale=-a.dt * gamma, add_mass=True, precision=cp.F32 if mixed else cp.F64)
     P = cp.BlockILU0(J, precision=cp.F32 if s_p == 4 else cp.F64)
     x = torch.randn(u.numel(), dtype=torch.float64, device="cuda")
@@ -437,12 +438,30 @@ def roofline(a, cp, ctx, eq, u, t, stream):
         t_mv = _timed(lambda: ctx.check(ctx._lib.cpg_bsr_matvec(ctx.h, J.h, cp.C.c_void_p(x.data_ptr()),
                                                                 cp.C.c_void_p(y.data_ptr()))), reps, stream)
         torch.cuda.nvtx.range_pop()
+        # the GMRES step's operator P^{-1} A as the solve takes it at its
+        # tolerance, and the split form whether or not it qualifies
+        xp, yp = cp.C.c_void_p(x.data_ptr()), cp.C.c_void_p(y.data_ptr())
+        torch.cuda.nvtx.range_push("roofline_operator")
+        t_op = _timed(lambda: ctx.check(ctx._lib.cpg_precond_apply_op(ctx.h, P.h, J.h, xp, yp, gmres_tol)),
+                      reps, stream)
+        torch.cuda.nvtx.range_pop()
+        t_split = None
+        if P.split_ready(J):
+            t_split = _timed(lambda: ctx.check(ctx._lib.cpg_precond_apply_op(ctx.h, P.h, J.h, xp, yp, 1.0)),
+                             reps, stream)
+        ctx.sync()
     finally:
         ctx.check(ctx._lib.cpg_ctx_set_deferred_checks(ctx.h, 0))
     form = int(ctx._lib.cpg_precond_sweep_form(P.h))
+    cond = P.pivot_cond()
+    split = P.split_ready(J) and 0.25 * 2.0 ** -52 * cond <= gmres_tol
     alg_sw = nnzb * bl * bl * s_p + 4 * n * bl * 8
     alg_mv = nnzb * bl * bl * s_a + 2 * n * bl * 8
     ach_sw, ach_mv = alg_sw / t_sw / 1e9, alg_mv / t_mv / 1e9
+    # split rows: E_i and A's upper blocks ((nnzb - n) / 2, symmetric
+    # pattern), x in, y out; the backward sweep also reads x once more
+    alg_sr = (n + (nnzb - n) // 2) * bl * bl * s_a + 2 * n * bl * 8
+    alg_op = (alg_sr + alg_sw + n * bl * 8) if split else (alg_mv + alg_sw)
     prec_sw = "FP32" if s_p == 4 else "FP64"
     kname = {1: "k_sweep (TMA ring)", 4: "k_sweep_direct", 5: "k_sweep_direct (2x rows)",
              6: "k_sweep_direct (4x rows)", 2: "k_rows per level", 3: "k_rows per level (wide)"}.get(form, "sweep")
@@ -456,7 +475,21 @@ def roofline(a, cp, ctx, eq, u, t, stream):
             "matvec": {"kernel": f"k_rows (BSR matvec, {bl}x{bl} {'FP32' if mixed else 'FP64'} blocks)",
                        "achieved": ach_mv, "frac": ach_mv / pk["hbm_gbs"], "algorithmic_bytes": alg_mv,
                        "launch_ms": t_mv * 1e3,
-                       "traffic": profiled_traffic(f"bsr_matvec_{'f32' if mixed else 'f64'}_bl{bl}.md")}}
+                       "traffic": profiled_traffic(f"bsr_matvec_{'f32' if mixed else 'f64'}_bl{bl}.md")},
+            "operator": {"kernel": ("P^{-1} A, split form: k_rows_split (E + upper blocks of A), forward sweep, "
+                                    "backward sweep adding x" if split else "P^{-1} A: BSR matvec, then ILU(0) apply"),
+                         "split": split, "pivot_cond_max": cond, "gmres_tol": gmres_tol,
+                         "launch_ms": t_op * 1e3, "algorithmic_bytes": alg_op,
+                         "achieved": alg_op / t_op / 1e9, "frac": alg_op / t_op / 1e9 / pk["hbm_gbs"]}}
+    if t_split is not None:
+        # the split form timed even where its rounding (eps * cond) keeps the
+        # solve on the plain product
+        alg_spl = alg_sr + alg_sw + n * bl * 8
+        t_sr = max(t_split - t_sw, 1e-9)
+        roof["operator"]["split_form"] = {"used_by_the_solve": split, "launch_ms": t_split * 1e3,
+                                          "algorithmic_bytes": alg_spl, "achieved": alg_spl / t_split / 1e9,
+                                          "split_rows_ms": t_sr * 1e3,
+                                          "split_rows_achieved": alg_sr / t_sr / 1e9}
     del P, J
     return roof
 

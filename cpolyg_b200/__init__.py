@@ -446,6 +446,23 @@ class Preconditioner:
         self.ctx.check(self._lib.cpg_precond_apply(self.ctx.h, self.h, C.c_void_p(_ptr(x))))
         return x
 
+    def apply_op(self, A: BlockMatrix, x, accuracy: float = 0.0):
+        """P^{-1} A x, the operator of a left-preconditioned GMRES step; the
+        split form when this is an FP64 ILU(0) of A's current values and
+        0.25 eps pivot_cond() <= accuracy (0: the plain product)."""
+        import torch
+        y = torch.empty_like(x)
+        self.ctx.check(self._lib.cpg_precond_apply_op(self.ctx.h, self.h, A.h, C.c_void_p(_ptr(x)),
+                                                      C.c_void_p(_ptr(y)), accuracy))
+        return y
+
+    def split_ready(self, A: BlockMatrix) -> bool:
+        return bool(self._lib.cpg_precond_split_ready(self.h, A.h))
+
+    def pivot_cond(self) -> float:
+        """largest cond_inf of a pivot block in the last factorisation"""
+        return float(self._lib.cpg_precond_pivot_cond(self.h))
+
     def levels(self):
         nl, nu = C.c_int(), C.c_int()
         self._lib.cpg_precond_levels(self.h, C.byref(nl), None, None, C.byref(nu), None, None)

@@ -115,6 +115,9 @@ PROTOTYPES = {
     "cpg_precond_refactor": (I, [P, P, P]),
     "cpg_precond_apply": (I, [P, P, P]),
     "cpg_precond_sweep_form": (I, [P]),
+    "cpg_precond_apply_op": (I, [P, P, P, P, P, D]),
+    "cpg_precond_split_ready": (I, [P, P]),
+    "cpg_precond_pivot_cond": (D, [P]),
     "cpg_debug_sweep_timeout": (I, [P]),
     "cpg_precond_destroy": (None, [P]),
     "cpg_precond_levels": (I, [P, PI, PI, PI, PI, PI, PI]),

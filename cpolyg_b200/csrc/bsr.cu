@@ -120,7 +120,7 @@ template <class T, int BL, int VEC, int TPR>
 __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, const int *__restrict__ rowptr,
                                               const int *__restrict__ col, const T *__restrict__ vals,
                                               const double *x, double *y, int mode, const int *skip,
-                                              int prefetch) {
+                                              int prefetch, const double *addv) {
     if (skip && *skip) return;  // a Krylov solve that has converged
     static_assert((TPR * VEC) % BL == 0, "stride must be a multiple of the block size");
     static_assert(BL % VEC == 0, "vector width must divide the block size");
@@ -169,6 +169,7 @@ __global__ void __launch_bounds__(TPR) k_rows(const int *__restrict__ rows, cons
         for (int q = 0; q < G; q++) s += red[q][tid];
         double *yi = y + (size_t)i * BL;
         if (mode == MODE_FORWARD) s = yi[tid] + s;
+        else if (addv) s = s + __ldg(addv + (size_t)i * BL + tid);
         yi[tid] = s;
     }
 }
@@ -178,7 +179,7 @@ template <class T>
 __global__ void __launch_bounds__(256) k_rows_dyn(int BL, int G, const int *__restrict__ rows,
                                                   const int *__restrict__ rowptr, const int *__restrict__ col,
                                                   const T *__restrict__ vals, const double *x, double *y, int mode,
-                                                  const int *skip) {
+                                                  const int *skip, const double *addv) {
     if (skip && *skip) return;
     extern __shared__ double red_dyn[];
     __shared__ int scol[MAX_ROW_BLOCKS];
@@ -215,6 +216,7 @@ __global__ void __launch_bounds__(256) k_rows_dyn(int BL, int G, const int *__re
         for (int q = 0; q < G; q++) s += red_dyn[q * BL + tid];
         double *yi = y + (size_t)i * BL;
         if (mode == MODE_FORWARD) s = yi[tid] + s;
+        else if (addv) s = s + __ldg(addv + (size_t)i * BL + tid);
         yi[tid] = s;
     }
 }
@@ -358,7 +360,8 @@ struct SweepSmem {
 template <class T, int BL>
 __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32)
     k_sweep(const int *__restrict__ order, int n, const int *__restrict__ rowptr, const int *__restrict__ col,
-            const T *__restrict__ vals, double *x, int mode, int *flags, int gen, int *counter, int *err, const int *skip) {
+            const T *__restrict__ vals, double *x, int mode, int *flags, int gen, int *counter, int *err, const int *skip,
+            const double *addv) {
     if (skip && *skip) return;  // a Krylov solve that has converged
     using Sh = SweepShape<T, BL>;
     using L = SweepSmem<T, BL>;
@@ -530,6 +533,7 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32)
                 for (int qq = 0; qq < G; qq++) s += red[qq][tid];
                 double *xi = x + (size_t)i * BL;
                 if (mode == MODE_FORWARD) s = __ldcg(xi + tid) + s;
+                else if (addv) s = s + __ldg(addv + (size_t)i * BL + tid);
                 __stcg(xi + tid, s);
             }
             consumers_sync(CT);  // also: nobody stages the next row's xs before this row is done
@@ -543,7 +547,8 @@ __global__ void __launch_bounds__(SweepShape<T, BL>::CT + 32)
 
 template <class T, int BL>
 cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
-                            const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err) {
+                            const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err,
+                            const double *addv) {
     using L = SweepSmem<T, BL>;
     constexpr int threads = SweepShape<T, BL>::CT + 32;
     static std::atomic<int> per_sm[64];  // occupancy per device, computed once
@@ -557,7 +562,7 @@ cpg_status launch_sweep_cfg(cpg_ctx *ctx, int nrows, const int *order, const int
     const int grid = std::max(1, std::min(nrows, std::max(1, occ) * ctx->num_sms));
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
     k_sweep<T, BL><<<grid, threads, L::BYTES, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags, gen,
-                                                            counter, err, ctx->skip_dev);
+                                                            counter, err, ctx->skip_dev, addv);
     return launched(ctx, "sync-free sweep kernel");
 }
 
@@ -576,7 +581,7 @@ template <class T, int BL, int TPR>
 __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
     k_sweep_direct(const int *__restrict__ order, int n, const int *__restrict__ rowptr,
                    const int *__restrict__ col, const T *__restrict__ vals, double *x, int mode, int *flags,
-                   int gen, int *counter, int *err, const int *skip, int prefetch) {
+                   int gen, int *counter, int *err, const int *skip, int prefetch, const double *addv) {
     if (skip && *skip) return;  // a Krylov solve that has converged
     constexpr int VEC = SweepShape<T, BL>::VEC;
     constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
@@ -651,6 +656,7 @@ __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
             for (int qq = 0; qq < G; qq++) sum += red[qq][tid];
             double *xi = x + (size_t)i * BL;
             if (mode == MODE_FORWARD) sum = __ldcg(xi + tid) + sum;
+            else if (addv) sum = sum + __ldg(addv + (size_t)i * BL + tid);
             __stcg(xi + tid, sum);
         }
         __syncthreads();  // the row's stores and the next claim are done
@@ -664,7 +670,7 @@ __global__ void __launch_bounds__(TPR, (1920 / TPR > 0 ? 1920 / TPR : 1))
 template <class T, int BL, int TPR>
 cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, const int *rowptr, const int *col,
                                    const T *vals, double *x, int mode, int *flags, int gen, int *counter,
-                                   int *err) {
+                                   int *err, const double *addv) {
     static std::atomic<int> per_sm[64];  // occupancy per device, computed once
     const bool cacheable = ctx->device >= 0 && ctx->device < 64;
     int occ = cacheable ? per_sm[ctx->device].load() : 0;
@@ -676,7 +682,7 @@ cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, co
     CPG_CUDA(ctx, cudaMemsetAsync(counter, 0, sizeof(int), ctx->stream));
     k_sweep_direct<T, BL, TPR><<<grid, TPR, 0, ctx->stream>>>(order, nrows, rowptr, col, vals, x, mode, flags,
                                                              gen, counter, err, ctx->skip_dev,
-                                                             nrows < PREFETCH_ROWS ? 1 : 0);
+                                                             nrows < PREFETCH_ROWS ? 1 : 0, addv);
     return launched(ctx, "sync-free sweep kernel (direct)");
 }
 
@@ -685,7 +691,7 @@ cpg_status launch_sweep_direct_cfg(cpg_ctx *ctx, int nrows, const int *order, co
 template <class T>
 cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, const int *rowptr, const int *col,
                           const T *vals, double *x, int mode, int *flags, int gen, int *counter, int *err,
-                          int kind) {
+                          int kind, const double *addv) {
     if (nrows <= 0) return CPG_OK;
 #define CPG_SWEEP(BLV)                                                                                          \
     {                                                                                                           \
@@ -693,16 +699,16 @@ cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, con
         switch (kind) {                                                                                         \
             case 1:                                                                                             \
                 return launch_sweep_direct_cfg<T, BLV, CT>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, \
-                                                           gen, counter, err);                                  \
+                                                           gen, counter, err, addv);                            \
             case 2:                                                                                             \
                 return launch_sweep_direct_cfg<T, BLV, 2 * CT>(ctx, nrows, order, rowptr, col, vals, x, mode,    \
-                                                               flags, gen, counter, err);                       \
+                                                               flags, gen, counter, err, addv);                 \
             case 3:                                                                                             \
                 return launch_sweep_direct_cfg<T, BLV, 4 * CT>(ctx, nrows, order, rowptr, col, vals, x, mode,    \
-                                                               flags, gen, counter, err);                       \
+                                                               flags, gen, counter, err, addv);                 \
             default:                                                                                            \
                 return launch_sweep_cfg<T, BLV>(ctx, nrows, order, rowptr, col, vals, x, mode, flags, gen,       \
-                                                counter, err);                                                  \
+                                                counter, err, addv);                                            \
         }                                                                                                       \
     }
     switch (bl) {
@@ -715,9 +721,96 @@ cpg_status launch_sweep_t(cpg_ctx *ctx, int bl, int nrows, const int *order, con
 #undef CPG_SWEEP
 }
 
+// ---------------------------------------------------------------------------
+// Rows of the split form of P^{-1} A for an ILU(0) P (precond.cu): with
+// A = (I + L) D + D U' + E, the product needs y = (U_A + E) x only, where
+// y_i = E_i x_i + sum_{j > i} A_ij x_j.  The columns are those of the DU
+// row (its first block is the row's own); E_i stands in for the D^{-1} slot
+// and the other blocks are read from A at the positions u2a.  Threads per
+// row and element order as k_rows.
+// ---------------------------------------------------------------------------
+template <int BL, int VEC, int TPR>
+__global__ void __launch_bounds__(TPR) k_rows_split(const int *__restrict__ rowptr, const int *__restrict__ col,
+                                                    const int *__restrict__ u2a, const double *__restrict__ vals,
+                                                    const double *__restrict__ Eb, const double *x, double *y,
+                                                    const int *skip, int prefetch) {
+    if (skip && *skip) return;  // a Krylov solve that has converged
+    static_assert((TPR * VEC) % BL == 0, "stride must be a multiple of the block size");
+    constexpr int S = TPR * VEC, G = S / BL, BL2 = BL * BL;
+    constexpr unsigned BYTES = BL2 * sizeof(double);
+    __shared__ int scol[SWEEP_MAXB];
+    __shared__ const double *sptr[SWEEP_MAXB];
+    __shared__ double red[G][BL];
+    const int i = blockIdx.x;
+    const int k0 = rowptr[i], nraw = rowptr[i + 1] - k0;
+    const int nblk = nraw > SWEEP_MAXB ? SWEEP_MAXB : nraw;  // the host admits no longer rows
+    const int tid = threadIdx.x;
+    for (int q = tid; q < nblk; q += TPR) {
+        const double *p = q == 0 ? Eb + (size_t)i * BL2 : vals + (size_t)u2a[k0 + q] * BL2;
+        scol[q] = col[k0 + q];
+        sptr[q] = p;
+        if constexpr (BYTES % 16 == 0)
+            if (prefetch)
+                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(BYTES) : "memory");
+    }
+    __syncthreads();
+    const int e0 = tid * VEC;
+    const int r0 = e0 % BL, g = e0 / BL;
+    double acc[VEC];
+#pragma unroll
+    for (int v = 0; v < VEC; v++) acc[v] = 0.0;
+    const int E = nblk * BL2;
+    int blk = e0 / BL2, within = e0 % BL2;
+#pragma unroll 4
+    for (int e = e0; e < E; e += S) {
+        const int c = within / BL;
+        double a[VEC];
+        VecLoad<double, VEC>::ld(sptr[blk] + within, a);
+        const double xv = __ldg(x + (size_t)scol[blk] * BL + c);
+#pragma unroll
+        for (int v = 0; v < VEC; v++) acc[v] += a[v] * xv;
+        within += S;
+        while (within >= BL2) {
+            within -= BL2;
+            blk++;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < VEC; v++) red[g][r0 + v] = acc[v];
+    __syncthreads();
+    if (tid < BL) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < G; q++) s += red[q][tid];
+        y[(size_t)i * BL + tid] = s;
+    }
+}
+
+cpg_status launch_split_v(cpg_ctx *ctx, int bl, int nrows, const int *rowptr, const int *col, const int *u2a,
+                          const double *vals, const double *E, const double *x, double *y, int variant) {
+    cudaStream_t s = ctx->stream;
+    const int pf = nrows < PREFETCH_ROWS ? 1 : 0;
+#define CPG_SPLIT3(BLV, T0, T1, T2)                                                                               \
+    switch (variant) {                                                                                            \
+        case 0: k_rows_split<BLV, 2, T0><<<nrows, T0, 0, s>>>(rowptr, col, u2a, vals, E, x, y, ctx->skip_dev, pf); break; \
+        case 1: k_rows_split<BLV, 2, T1><<<nrows, T1, 0, s>>>(rowptr, col, u2a, vals, E, x, y, ctx->skip_dev, pf); break; \
+        default: k_rows_split<BLV, 2, T2><<<nrows, T2, 0, s>>>(rowptr, col, u2a, vals, E, x, y, ctx->skip_dev, pf); break; \
+    }
+    switch (bl) {
+        case 6: CPG_SPLIT3(6, 96, 192, 384) break;
+        case 10: CPG_SPLIT3(10, 160, 320, 640) break;
+        case 24: CPG_SPLIT3(24, 192, 384, 576) break;
+        case 40: CPG_SPLIT3(40, 160, 320, 640) break;
+        default: return fail(ctx, CPG_ERR_UNSUPPORTED, "block size of the split rows");
+    }
+#undef CPG_SPLIT3
+    return launched(ctx, "split block-row kernel");
+}
+
 template <class T>
 cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const int *rowptr, const int *col,
-                         const T *vals, const double *x, double *y, int mode, int variant) {
+                         const T *vals, const double *x, double *y, int mode, int variant,
+                         const double *addv) {
     if (nrows <= 0) return CPG_OK;
     cudaStream_t s = ctx->stream;
     constexpr bool F32 = std::is_same<T, float>::value;
@@ -730,19 +823,19 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
     // the widest variant because they are latency bound
 #define CPG_ROWS3(BLV, V, T0, T1, T2)                                                                    \
     switch (variant) {                                                                                   \
-        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;  \
-        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;  \
-        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break; \
+        case 0: k_rows<T, BLV, V, T0><<<nrows, T0, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv); break;  \
+        case 1: k_rows<T, BLV, V, T1><<<nrows, T1, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv); break;  \
+        default: k_rows<T, BLV, V, T2><<<nrows, T2, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv); break; \
     }
     switch (bl) {
-        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;
-        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;
-        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf); break;
+        case 1: k_rows<T, 1, 1, 32><<<nrows, 32, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv); break;
+        case 3: k_rows<T, 3, 1, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv); break;
+        case 4: k_rows<T, 4, 2, 64><<<nrows, 64, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv); break;
         case 6: CPG_ROWS3(6, 2, 96, 192, 384) break;
         case 10: CPG_ROWS3(10, 2, 160, 320, 640) break;
         case 12:
-            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf);
-            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf);
+            if constexpr (F32) k_rows<T, 12, 4, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv);
+            else k_rows<T, 12, 2, 96><<<nrows, 96, 0, s>>>(rows, rowptr, col, vals, x, y, mode, ctx->skip_dev, pf, addv);
             break;
         case 24:
             if constexpr (F32) { CPG_ROWS3(24, 4, 96, 192, 288) }
@@ -760,7 +853,7 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
             if (bl > 256) return fail(ctx, CPG_ERR_UNSUPPORTED, "block size above 256");
             const int G = std::max(1, 256 / bl);
             k_rows_dyn<T><<<nrows, 256, sizeof(double) * bl * G, s>>>(bl, G, rows, rowptr, col, vals, x, y, mode,
-                                                                     ctx->skip_dev);
+                                                                     ctx->skip_dev, addv);
         }
     }
 #undef CPG_ROWS3
@@ -768,10 +861,13 @@ cpg_status launch_rows_t(cpg_ctx *ctx, int bl, int nrows, const int *rows, const
 }
 
 cpg_status launch_rows_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
-                         const int *col, const void *vals, const double *x, double *y, int mode, int variant) {
+                         const int *col, const void *vals, const double *x, double *y, int mode, int variant,
+                         const double *addv = nullptr) {
     if (precision == CPG_F32)
-        return launch_rows_t<float>(ctx, bl, nrows, rows, rowptr, col, (const float *)vals, x, y, mode, variant);
-    return launch_rows_t<double>(ctx, bl, nrows, rows, rowptr, col, (const double *)vals, x, y, mode, variant);
+        return launch_rows_t<float>(ctx, bl, nrows, rows, rowptr, col, (const float *)vals, x, y, mode, variant,
+                                    addv);
+    return launch_rows_t<double>(ctx, bl, nrows, rows, rowptr, col, (const double *)vals, x, y, mode, variant,
+                                 addv);
 }
 
 // ---------------------------------------------------------------------------
@@ -825,6 +921,45 @@ int tuned_variant(cpg_ctx *ctx, int precision, int bl, int nrows, const int *row
     return best;
 }
 
+// the split rows' own threads-per-row decision per block size, taken the
+// same way on the first split product of the process
+int g_tune_split[64];
+
+int tuned_split_variant(cpg_ctx *ctx, int bl, int nrows, const int *rowptr, const int *col, const int *u2a,
+                        const double *vals, const double *E, const double *x, double *y) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    if (g_tune_split[bl]) return g_tune_split[bl] - 1;
+    const char *env = std::getenv("CPG_AUTOTUNE");
+    if ((env && std::strcmp(env, "0") == 0) || nrows < 2048) return 0;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return 0;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return 0;
+    }
+    int best = 0;
+    float best_ms = 1e30f;
+    for (int v = 0; v < 3; v++) {
+        bool ok = true;
+        for (int r = 0; r < 2 && ok; r++)
+            ok = launch_split_v(ctx, bl, nrows, rowptr, col, u2a, vals, E, x, y, v) == CPG_OK;
+        cudaEventRecord(e0, ctx->stream);
+        for (int r = 0; r < 3 && ok; r++)
+            ok = launch_split_v(ctx, bl, nrows, rowptr, col, u2a, vals, E, x, y, v) == CPG_OK;
+        cudaEventRecord(e1, ctx->stream);
+        float ms = 1e30f;
+        if (ok && cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        if (ok && ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    g_tune_split[bl] = best + 1;
+    return best;
+}
+
 cpg_status launch_rows(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
                        const int *col, const void *vals, const double *x, double *y, int mode) {
     // level sweeps: variant 0, the threads per row of the sync-free sweep's
@@ -843,24 +978,38 @@ cpg_status rows_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *ro
     return launch_rows(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode);
 }
 cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
-                     const int *col, const void *vals, const double *x, double *y, int mode, int variant) {
-    return launch_rows_v(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode, variant);
+                     const int *col, const void *vals, const double *x, double *y, int mode, int variant,
+                     const double *addv) {
+    return launch_rows_v(ctx, precision, bl, nrows, rows, rowptr, col, vals, x, y, mode, variant, addv);
 }
 bool rows_tunable(int bl) { return tunable(bl); }
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
-                    int *err, int kind) {
+                    int *err, int kind, const double *addv) {
     if (precision == CPG_F32)
         return launch_sweep_t<float>(ctx, bl, nrows, order, rowptr, col, (const float *)vals, x, mode, flags, gen,
-                                     counter, err, kind);
+                                     counter, err, kind, addv);
     return launch_sweep_t<double>(ctx, bl, nrows, order, rowptr, col, (const double *)vals, x, mode, flags, gen,
-                                  counter, err, kind);
+                                  counter, err, kind, addv);
 }
 bool sweep_supported(int bl) { return bl == 6 || bl == 10 || bl == 24 || bl == 40; }
 cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y) {
     return launch_rows(ctx, A->precision, A->bl, A->n_rows, nullptr, A->rowptr_d, A->colidx_d, A->vals, x, y,
                        MODE_MATVEC);
 }
+cpg_status split_rows_op(cpg_ctx *ctx, const cpg_bsr *A, const int *U_rowptr, const int *U_col, const int *u2a,
+                         const double *E, const double *x, double *y) {
+    if (A->precision != CPG_F64) return fail(ctx, CPG_ERR_UNSUPPORTED, "split rows need FP64 values");
+    const int n = A->n_rows;
+    if (n <= 0) return CPG_OK;
+    const double *vals = (const double *)A->vals;
+    const int v = tuned_split_variant(ctx, A->bl, n, U_rowptr, U_col, u2a, vals, E, x, y);
+    return launch_split_v(ctx, A->bl, n, U_rowptr, U_col, u2a, vals, E, x, y, v);
+}
+// stamps come from one process-wide counter, so a matrix freed and another
+// allocated at the same address never share one
+std::atomic<uint64_t> g_bsr_version{0};
+void bsr_touch(cpg_bsr *A) { A->version = ++g_bsr_version; }
 }  // namespace cpg
 
 static void free_bsr(cpg_bsr *A) {
@@ -882,6 +1031,7 @@ static cpg_status bsr_alloc(cpg_ctx *ctx, cpg_bsr *A) {
         return fail(ctx, CPG_ERR_OOM, "BSR values: cudaMalloc of " + std::to_string(bytes) + " bytes failed");
     }
     CPG_CUDA(ctx, cudaMemsetAsync(A->vals, 0, bytes, ctx->stream));
+    bsr_touch(A);
     return CPG_OK;
 }
 
@@ -983,6 +1133,7 @@ cpg_status cpg_bsr_upload(cpg_ctx *ctx, cpg_bsr *A, const double *values_host) {
         CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         cudaFree(tmp);
     }
+    bsr_touch(A);
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return CPG_OK;
 }
@@ -1017,6 +1168,7 @@ cpg_status cpg_bsr_stack(cpg_ctx *ctx, int k, const cpg_bsr *const *parts, cpg_b
         }
         at += bytes;
     }
+    bsr_touch(S);
     *out = S;
     return CPG_OK;
 }

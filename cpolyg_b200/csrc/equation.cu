@@ -839,6 +839,7 @@ cpg_status cpg_jacobian(cpg_ctx *ctx, const cpg_equation *eq, const double *u, d
             k_jacobian<decltype(ph), P, double><<<eq->n, JT, 0, ctx->stream>>>(
                 eq->geo(), ph, eq->bc, u, t, scale, add_mass, eq->mass, eq->rowptr_d, (double *)J->vals);
         }
+        bsr_touch(J);
         return launched(ctx, "jacobian kernel");
     });
 }

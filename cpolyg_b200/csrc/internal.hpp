@@ -62,6 +62,9 @@ struct cpg_bsr {
     int *rowptr_d = nullptr, *colidx_d = nullptr;
     void *vals = nullptr;              // double or float, nnzb * bl * bl
     bool owns_pattern = true;
+    // process-unique stamp of the values, renewed by every write through the
+    // library (cpg::bsr_touch); a factorisation records the stamp it read
+    uint64_t version = 0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
 };
 
@@ -101,6 +104,19 @@ struct cpg_precond {
     int n_cand = 0, cand[6] = {0, 0, 0, 0, 0, 0};
     int form_key = -1;  // process-wide key of the decision (block size, precision, size class)
     int64_t nnzL = 0, nnzU = 0;
+    // split form of M^{-1} A (FP64 ILU(0) only): E_i = A_ii - Ahat_ii per
+    // row, the A position of every upper block of a DU row (u2a, -1 at the
+    // D^{-1} slot), and the matrix and value stamp the factors were built
+    // from; the split form applies only to that matrix with that stamp
+    double *E_vals = nullptr;
+    int *u2a_d = nullptr;
+    bool split_capable = false;
+    const cpg_bsr *split_src = nullptr;
+    uint64_t split_version = 0;
+    // largest cond_inf of a pivot block in the last factorisation (device
+    // word as the bits of a non-negative double, and its host copy)
+    unsigned long long *cond_d = nullptr;
+    double pivot_cond = 0.0;
     size_t elem() const { return precision == CPG_F32 ? sizeof(float) : sizeof(double); }
 };
 
@@ -109,8 +125,15 @@ namespace cpg {
 struct LinOp {
     virtual cpg_status apply(cpg_ctx *ctx, const double *x, double *y) const = 0;  // y = A x
     virtual cpg_status prec(cpg_ctx *ctx, double *x) const = 0;                    // x = P^{-1} x
+    // y = P^{-1} A x (x and y distinct)
+    virtual cpg_status apply_prec(cpg_ctx *ctx, const double *x, double *y) const {
+        const cpg_status st = apply(ctx, x, y);
+        return st == CPG_OK ? prec(ctx, y) : st;
+    }
     virtual ~LinOp() {}
 };
+// renews A's value stamp after a write to its values (bsr.cu)
+void bsr_touch(cpg_bsr *A);
 cpg_status gmres_op(cpg_ctx *ctx, const LinOp &op, int64_t N, const double *b, double *x, int m, double tol,
                     int maxit, int flexible, cpg_solve_stats *stats);
 // residual kernel alone, without the state check of cpg_assemble (equation.cu)
@@ -123,17 +146,29 @@ cpg_status mass_solve_scaled(cpg_ctx *ctx, const cpg_equation *eq, const double 
 cpg_status bsr_matvec_raw(cpg_ctx *ctx, const cpg_bsr *A, const double *x, double *y);
 // sync-free triangular sweep over the rows in `order` (bsr.cu)
 // block-row kernel with an explicit threads-per-row variant (bsr.cu)
+// addv (or null): added to every row's result of a backward sweep
 cpg_status rows_op_v(cpg_ctx *ctx, int precision, int bl, int nrows, const int *rows, const int *rowptr,
-                     const int *col, const void *vals, const double *x, double *y, int mode, int variant);
+                     const int *col, const void *vals, const double *x, double *y, int mode, int variant,
+                     const double *addv = nullptr);
 bool rows_tunable(int bl);
 cpg_status sweep_op(cpg_ctx *ctx, int precision, int bl, int nrows, const int *order, const int *rowptr,
                     const int *col, const void *vals, double *x, int mode, int *flags, int gen, int *counter,
-                    int *err, int kind = 0);
+                    int *err, int kind = 0, const double *addv = nullptr);
+// y_i = E_i x_i + sum_{j > i} A_ij x_j over the DU rows' columns, with the
+// A positions u2a and the row blocks E (FP64 values; bsr.cu)
+cpg_status split_rows_op(cpg_ctx *ctx, const cpg_bsr *A, const int *U_rowptr, const int *U_col, const int *u2a,
+                         const double *E, const double *x, double *y);
 bool sweep_supported(int bl);
 constexpr int SWEEP_MAX_ROW_BLOCKS = 16;  // longest L or DU row the sync-free sweep takes
 // x = P^{-1} x without the host-side check of the sweep status word, for
 // callers that check once per solve (precond.cu)
-cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x);
+cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x, const double *addv = nullptr);
+// P is an FP64 ILU(0) factored from A's current values (precond.cu)
+bool split_ready(const cpg_precond *P, const cpg_bsr *A);
+// ... and the split form's rounding stays well below tol
+bool split_allowed(const cpg_precond *P, const cpg_bsr *A, double tol);
+// y = P^{-1} A x in split form (the caller checked split_allowed)
+cpg_status split_apply_prec(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const double *x, double *y);
 // reads and clears the sweep status word; a bounded wait that ran out turns
 // `st` into CPG_ERR_TIMEOUT (precond.cu)
 cpg_status check_sweep_error(cpg_ctx *ctx, cpg_status st);

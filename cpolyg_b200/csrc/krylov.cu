@@ -170,9 +170,14 @@ cpg_status vec_dot(cpg_ctx *ctx, int64_t n, const double *x, const double *y, do
 struct KrylovOp : LinOp {
     const cpg_bsr *A;
     const cpg_precond *P;
-    KrylovOp(const cpg_bsr *a, const cpg_precond *p) : A(a), P(p) {}
+    bool split;  // P^{-1} A in split form (an FP64 ILU(0) of A's current values, rounding well below tol)
+    KrylovOp(const cpg_bsr *a, const cpg_precond *p, double tol) : A(a), P(p), split(split_allowed(p, a, tol)) {}
     cpg_status apply(cpg_ctx *ctx, const double *x, double *y) const override { return bsr_matvec_raw(ctx, A, x, y); }
     cpg_status prec(cpg_ctx *ctx, double *x) const override { return precond_apply_raw(ctx, P, x); }
+    cpg_status apply_prec(cpg_ctx *ctx, const double *x, double *y) const override {
+        if (split) return split_apply_prec(ctx, A, P, x, y);
+        return LinOp::apply_prec(ctx, x, y);
+    }
 };
 
 namespace {
@@ -488,8 +493,7 @@ cpg_status gmres_seg_run(cpg_ctx *ctx, const LinOp &op, int K, const int64_t *of
         for (int i = 0; i < m && rc == CPG_OK; i++) {
             double *vi = V + (size_t)N * i, *vi1 = V + (size_t)N * (i + 1);
             if (!flexible) {
-                rc = op.apply(ctx, vi, vi1);
-                if (rc == CPG_OK) rc = op.prec(ctx, vi1);
+                rc = op.apply_prec(ctx, vi, vi1);
             } else {
                 double *zi = Z + (size_t)N * i;
                 rc = vec_copy(ctx, N, vi, zi);
@@ -575,7 +579,7 @@ cpg_status cpg_gmres(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const
                      double tol, int maxit, int flexible, cpg_solve_stats *stats) {
     if (!ctx || !A || !b || !x || maxit < 1) return CPG_ERR_INVALID_ARG;
     if (P && (P->n != A->n_rows || P->bl != A->bl)) return fail(ctx, CPG_ERR_INVALID_ARG, "preconditioner size");
-    KrylovOp op(A, P);
+    KrylovOp op(A, P, tol);
     return gmres_op(ctx, op, (int64_t)A->n_rows * A->bl, b, x, m, tol, maxit, flexible, stats);
 }
 
@@ -600,7 +604,7 @@ cpg_status cpg_gmres_batched(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *
                     return fail(ctx, CPG_ERR_INVALID_ARG,
                                 "block (" + std::to_string(i) + ", " + std::to_string(A->colidx[q]) +
                                     ") couples two systems");
-    KrylovOp op(A, P);
+    KrylovOp op(A, P, tol);
     return check_sweep_error(ctx, gmres_seg_run(ctx, op, nsys, off.data(), b, x, m, tol, maxit, flexible, stats));
 }
 

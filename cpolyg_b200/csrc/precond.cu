@@ -15,7 +15,9 @@
 // in level order, per-row publish flags; block sizes 6, 10, 24, 40) or as one
 // launch per level (other block sizes, or CPG_ILU_SWEEP=levels).
 #include <algorithm>
+#include <cfloat>
 #include <climits>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -374,7 +376,8 @@ __global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__re
                                                    const int *__restrict__ lp_aij, const int *__restrict__ lp_l,
                                                    const int *__restrict__ lp_u, TS *__restrict__ Lv,
                                                    TS *Uv, const int *__restrict__ U_rowptr,
-                                                   double *dinv, const int *__restrict__ dinv_idx, int *flag) {
+                                                   double *dinv, const int *__restrict__ dinv_idx, int *flag,
+                                                   double *__restrict__ Eout) {
     extern __shared__ double sm[];
     const int BL = BLC ? BLC : bl_rt;
     const int BL2 = BL * BL;
@@ -413,6 +416,11 @@ __global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__re
         __syncthreads();
         // Ahat_jj goes to its D^{-1} slot; k_block_inverse inverts it in place
         store_pad<BLC>(Ap, dinv + (size_t)dinv_idx[j] * b2);
+        if (Eout) {  // E_j = A_jj - Ahat_jj for the split form of P^{-1} A
+            const TA *ajj = A + (size_t)diag_a[j] * b2;
+            for (int o = threadIdx.x; o < BL2; o += FT)
+                Eout[(size_t)j * b2 + o] = (double)ajj[o] - Ap[Pad<BLC>::at(o)];
+        }
         return;
     } else if constexpr (BLC > 0) {  // compiled-in sizes not divisible by 8: scalar products
         constexpr int PER = (BLC * BLC + FT - 1) / FT;
@@ -463,6 +471,24 @@ __global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__re
     // Ahat_jj goes to its D^{-1} slot; k_block_inverse inverts it in place
     double *dj = dinv + (size_t)dinv_idx[j] * b2;
     for (int o = threadIdx.x; o < BL2; o += FT) dj[o] = Ah[o];
+    if (Eout) {  // E_j = A_jj - Ahat_jj for the split form of P^{-1} A
+        const TA *ajj = A + (size_t)diag_a[j] * b2;
+        for (int o = threadIdx.x; o < BL2; o += FT) Eout[(size_t)j * b2 + o] = (double)ajj[o] - Ah[o];
+    }
+}
+
+// max over rows of sum_c |B(r, c)| for a column-major BL x BL block in
+// shared memory (lanes over rows: consecutive addresses), on every lane
+__device__ __forceinline__ double warp_norm_inf(int BL, const double *B) {
+    double m = 0.0;
+    for (int r = threadIdx.x & 31; r < BL; r += 32) {
+        double sum = 0.0;
+        for (int c = 0; c < BL; c++) sum += fabs(B[(size_t)c * BL + r]);
+        m = fmax(m, sum);
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, off));
+    return m;
 }
 
 // The level's pivot blocks, one warp each: Ahat_jj (FP64, in its D^{-1}
@@ -472,7 +498,8 @@ __global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__re
 template <class TS, int BLC>
 __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, const int *__restrict__ rows,
                                                        TS *Uv, const int *__restrict__ U_rowptr, double *dinv,
-                                                       const int *__restrict__ dinv_idx, int *flag) {
+                                                       const int *__restrict__ dinv_idx, int *flag,
+                                                       unsigned long long *cond_max) {
     extern __shared__ double sm[];
     const int BL = BLC ? BLC : bl_rt;
     const size_t b2 = (size_t)BL * BL;
@@ -490,6 +517,7 @@ __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, con
     double *dj = dinv + (size_t)dinv_idx[j] * b2;
     for (int o = lane; o < (int)b2; o += 32) A[o] = dj[o];
     __syncwarp();
+    const double nrm_a = warp_norm_inf(BL, A);  // before the inversion overwrites A
     bool ok;
     const double *Di;
     if constexpr (PANEL) {
@@ -502,6 +530,11 @@ __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, con
         atomicExch(flag, 1);
         atomicMin(flag + 1, j);
     }
+    // cond_inf(Ahat_jj) = |Ahat_jj|_inf |Ahat_jj^{-1}|_inf (the inverse's row
+    // sums do not depend on the column order perm); the largest over all
+    // pivot blocks, by the ordering of non-negative doubles' bit patterns
+    const double cond = nrm_a * warp_norm_inf(BL, Di);
+    if (ok && lane == 0 && cond_max) atomicMax(cond_max, (unsigned long long)__double_as_longlong(cond));
     TS *uj = Uv + (size_t)U_rowptr[j] * b2;
     const bool both = (void *)uj != (void *)dj;
     for (int c = 0; c < BL; c++) {
@@ -765,7 +798,7 @@ cpg_status launch_factor_tc(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     const size_t ismem = per_warp * wpb;
     CPG_TRY(smem_limit_once(ctx, (const void *)k_block_inverse<float, 40>, (int)ismem));
     k_block_inverse<float, 40><<<(nrows + wpb - 1) / wpb, 32 * wpb, ismem, ctx->stream>>>(
-        BL, nrows, rows, (float *)P->U_vals, P->U_rowptr_d, P->dinv64, P->dinv_idx_d, ctx->flag_dev);
+        BL, nrows, rows, (float *)P->U_vals, P->U_rowptr_d, P->dinv64, P->dinv_idx_d, ctx->flag_dev, P->cond_d);
     return launched(ctx, "pivot block inverse kernel");
 }
 
@@ -785,9 +818,12 @@ cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
                             BLC > 0 ? (int)smem : (smem > 48 * 1024 ? 227 * 1024 : 0)));
     if (smem > 227 * 1024) return fail(ctx, CPG_ERR_UNSUPPORTED, "block too large for the factor kernel");
     double *dinv = P->precision == CPG_F64 ? (double *)P->U_vals : P->dinv64;
+    // E_j for the split form: FP64 values and FP64 factors only
+    constexpr bool F64 = std::is_same<TA, double>::value && std::is_same<TS, double>::value;
+    double *E = (F64 && P->split_capable) ? P->E_vals : nullptr;
     k_ilu_factor<TA, TS, BLC><<<nrows, FT, smem, ctx->stream>>>(
         BL, rows, (const TA *)A->vals, P->diag_a_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d, P->lp_l_d,
-        P->lp_u_d, (TS *)P->L_vals, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
+        P->lp_u_d, (TS *)P->L_vals, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev, E);
     CPG_TRY(launched(ctx, "ilu factor kernel"));
     // pivot-block inverses: up to 4 warps per CTA within 110 KB of shared memory
     constexpr bool PANEL = BLC > 0 && BLC % 8 == 0;
@@ -799,7 +835,7 @@ cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     CPG_TRY(smem_limit_once(ctx, (const void *)k_block_inverse<TS, BLC>,
                             BLC > 0 ? (int)ismem : (ismem > 48 * 1024 ? 227 * 1024 : 0)));
     k_block_inverse<TS, BLC><<<(nrows + wpb - 1) / wpb, 32 * wpb, ismem, ctx->stream>>>(
-        BL, nrows, rows, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev);
+        BL, nrows, rows, (TS *)P->U_vals, P->U_rowptr_d, dinv, P->dinv_idx_d, ctx->flag_dev, P->cond_d);
     return launched(ctx, "pivot block inverse kernel");
 }
 
@@ -827,7 +863,7 @@ cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrow
 void free_precond(cpg_precond *P) {
     void *ptrs[] = {P->lrows_d, P->urows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, P->U_rowptr_d, P->U_col_d,
                     P->U_vals, P->dinv64, P->dinv_idx_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d,
-                    P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d};
+                    P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d, P->E_vals, P->u2a_d, P->cond_d};
     for (void *p : ptrs) dfree(p);
 }
 
@@ -837,17 +873,17 @@ namespace cpg {
 
 namespace sweep_form {
 
-cpg_status apply_syncfree(cpg_ctx *ctx, const cpg_precond *P, double *x, int kind) {
+cpg_status apply_syncfree(cpg_ctx *ctx, const cpg_precond *P, double *x, int kind, const double *addv) {
     // status word: flag_dev[2] = a wait ran out, flag_dev[4] = row counter
     int *err = ctx->flag_dev + 2, *counter = ctx->flag_dev + 4;
     const int g = ++P->generation;
     CPG_TRY(sweep_op(ctx, P->precision, P->bl, P->n, P->lrows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, x,
                      MODE_FORWARD, P->row_flags_d, 2 * g - 1, counter, err, kind));
     return sweep_op(ctx, P->precision, P->bl, P->n, P->urows_d, P->U_rowptr_d, P->U_col_d, P->U_vals, x,
-                    MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err, kind);
+                    MODE_BACKWARD, P->row_flags_d, 2 * g, counter, err, kind, addv);
 }
 
-cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x, int variant) {
+cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x, int variant, const double *addv) {
     if (P->kind == CPG_PC_ILU0) {
         const int nl = (int)P->lptr.size() - 1;
         for (int l = 0; l < nl; l++) {
@@ -861,15 +897,16 @@ cpg_status apply_levels(cpg_ctx *ctx, const cpg_precond *P, double *x, int varia
     for (int l = 0; l < nu; l++) {
         const int cnt = P->uptr[l + 1] - P->uptr[l];
         CPG_TRY(rows_op_v(ctx, P->precision, P->bl, cnt, P->urows_d + P->uptr[l], P->U_rowptr_d, P->U_col_d,
-                          P->U_vals, x, x, MODE_BACKWARD, variant));
+                          P->U_vals, x, x, MODE_BACKWARD, variant, addv));
     }
     return CPG_OK;
 }
 
-cpg_status apply_form(cpg_ctx *ctx, const cpg_precond *P, double *x, int form) {
-    if (form == 1) return apply_syncfree(ctx, P, x, 0);
-    if (form >= 4) return apply_syncfree(ctx, P, x, form - 3);
-    return apply_levels(ctx, P, x, form == 3 ? 2 : 0);
+// addv (or null) is added to every row of the backward sweep
+cpg_status apply_form(cpg_ctx *ctx, const cpg_precond *P, double *x, int form, const double *addv) {
+    if (form == 1) return apply_syncfree(ctx, P, x, 0, addv);
+    if (form >= 4) return apply_syncfree(ctx, P, x, form - 3, addv);
+    return apply_levels(ctx, P, x, form == 3 ? 2 : 0, addv);
 }
 
 // process-wide decisions, so every preconditioner of one kind, block size,
@@ -883,7 +920,7 @@ std::map<int, int> g_form;
 // for every preconditioner of the same class in the process.  The caller's
 // vector only ever sees the decided form, so a solve's result does not
 // depend on whether it was the one that timed the forms.
-cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x, const double *addv) {
     const size_t N = (size_t)P->n * P->bl;
     double *tmp = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -901,7 +938,7 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
                 timed = false;
                 break;
             }
-            st = apply_form(ctx, P, tmp, P->cand[c]);
+            st = apply_form(ctx, P, tmp, P->cand[c], addv);
             if (st == CPG_OK && cudaEventRecord(e1, ctx->stream) == cudaSuccess &&
                 cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
                 best_ms[c] = std::min(best_ms[c], ms);
@@ -924,7 +961,7 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
         // nothing was timed (no scratch memory for the copy, or every
         // candidate gave up): apply the level form this once and decide at a
         // later application rather than record an untimed choice
-        return apply_form(ctx, P, x, 2);
+        return apply_form(ctx, P, x, 2, addv);
     }
     {
         std::lock_guard<std::mutex> lk(g_form_mu);
@@ -932,7 +969,7 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x) {
         if (it == g_form.end()) g_form[P->form_key] = P->cand[best];
         P->sweep_mode = g_form[P->form_key];  // a concurrent first decision wins
     }
-    return apply_form(ctx, P, x, P->sweep_mode);
+    return apply_form(ctx, P, x, P->sweep_mode, addv);
 }
 
 // the candidates of a new preconditioner, or its form when already decided
@@ -978,10 +1015,41 @@ void choose_form(cpg_precond *P, const char *env) {
 
 }  // namespace sweep_form
 
-cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x) {
+cpg_status precond_apply_raw(cpg_ctx *ctx, const cpg_precond *P, double *x, const double *addv) {
     if (!P || P->kind == CPG_PC_NONE) return CPG_OK;
-    if (P->sweep_mode == 0) return sweep_form::apply_tuning(ctx, P, x);
-    return sweep_form::apply_form(ctx, P, x, P->sweep_mode);
+    if (P->sweep_mode == 0) return sweep_form::apply_tuning(ctx, P, x, addv);
+    return sweep_form::apply_form(ctx, P, x, P->sweep_mode, addv);
+}
+
+// Split form of P^{-1} A for P = (I + L) D (I + U') factored from A, where
+// L = L_A D^{-1} and U' = D^{-1} U_A hold A's strictly lower and upper
+// blocks.  Then A = (I + L) D + D U' + E with E_i = A_ii - Ahat_ii, and
+//   P^{-1} A x = (I + U')^{-1} [x + D^{-1} (I + L)^{-1} (U_A + E) x],
+// so one product reads A's upper blocks and E (split_rows_op), the forward
+// sweep runs as usual and the backward sweep adds x to every row.  Per
+// Krylov step that streams the upper part of A and E instead of all of A.
+//
+// The identity holds for the stored factors only up to their rounding:
+// L D - L_A, D U' - U_A and E - (A_ii - D_i) are each of order
+// eps * cond(D_i) |A|, so the split product is the plain one of a matrix
+// perturbed by that much (measured: 0.01 to 0.08 eps * max cond_inf(D_i),
+// relative).  A solve takes it only while that stays well below its
+// tolerance: SPLIT_ROUNDING * eps * max cond_inf(D_i) <= tol.
+constexpr double SPLIT_ROUNDING = 0.25;
+
+bool split_ready(const cpg_precond *P, const cpg_bsr *A) {
+    return P && A && P->kind == CPG_PC_ILU0 && P->split_capable && P->split_src == A &&
+           P->split_version == A->version && A->precision == CPG_F64 && P->precision == CPG_F64;
+}
+
+bool split_allowed(const cpg_precond *P, const cpg_bsr *A, double tol) {
+    return split_ready(P, A) && P->pivot_cond > 0.0 && std::isfinite(P->pivot_cond) &&
+           SPLIT_ROUNDING * DBL_EPSILON * P->pivot_cond <= tol;
+}
+
+cpg_status split_apply_prec(cpg_ctx *ctx, const cpg_bsr *A, const cpg_precond *P, const double *x, double *y) {
+    CPG_TRY(split_rows_op(ctx, A, P->U_rowptr_d, P->U_col_d, P->u2a_d, P->E_vals, x, y));
+    return precond_apply_raw(ctx, P, y, x);
 }
 
 cpg_status check_sweep_error(cpg_ctx *ctx, cpg_status st) {
@@ -1019,7 +1087,7 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     }
     const int n = A->n_rows;
     const std::vector<int> &rp = A->rowptr, &cl = A->colidx;
-    std::vector<int> diag_a(n, -1), a2l(A->nnzb, -1), a2u(A->nnzb, -1);
+    std::vector<int> diag_a(n, -1), a2l(A->nnzb, -1), a2u(A->nnzb, -1), u2a;
     const bool ilu = kind == CPG_PC_ILU0;
     P->L_rowptr.assign(1, 0);
     P->U_rowptr.assign(1, 0);
@@ -1047,6 +1115,7 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
         }
         // DU row: D^{-1} first, then upper blocks in A's row order
         P->U_col.push_back(i);
+        u2a.push_back(-1);
         if (ilu) {
             for (int k = rp[i]; k < rp[i + 1]; k++) {
                 if (cl[k] < i) {
@@ -1055,6 +1124,7 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
                 } else if (cl[k] > i) {
                     a2u[k] = (int)P->U_col.size();
                     P->U_col.push_back(cl[k]);
+                    u2a.push_back(k);
                 }
             }
         }
@@ -1114,6 +1184,10 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     for (int i = 0; i < n; i++)
         longest = std::max({longest, P->L_rowptr[i + 1] - P->L_rowptr[i], P->U_rowptr[i + 1] - P->U_rowptr[i]});
     P->syncfree = ilu && sweep_supported(P->bl) && !level_sweeps && longest <= SWEEP_MAX_ROW_BLOCKS;
+    // the split form of P^{-1} A (FP64 values and factors); CPG_SPLIT_OPERATOR=0 turns it off
+    const char *split_env = std::getenv("CPG_SPLIT_OPERATOR");
+    P->split_capable = ilu && precision == CPG_F64 && A->precision == CPG_F64 && sweep_supported(P->bl) &&
+                       longest <= SWEEP_MAX_ROW_BLOCKS && !(split_env && std::strcmp(split_env, "0") == 0);
     sweep_form::choose_form(P, sweep_env);
     cpg_status st = CPG_OK;
     if (P->syncfree) {
@@ -1140,6 +1214,11 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
     up(&P->lp_u_d, lp_u);
     up(&P->diag_a_d, diag_a);
     up(&P->dinv_idx_d, dinv_idx);
+    if (st == CPG_OK) st = dmalloc(ctx, &P->cond_d, 1);
+    if (P->split_capable) {
+        up(&P->u2a_d, u2a);
+        if (st == CPG_OK) st = dmalloc(ctx, &P->E_vals, (size_t)n * P->bl * P->bl);
+    }
     const size_t b2 = (size_t)P->bl * P->bl;
     if (st == CPG_OK && P->nnzL) {
         cudaError_t e = cudaMalloc(&P->L_vals, P->nnzL * b2 * P->elem());
@@ -1164,17 +1243,27 @@ cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A) 
     if (!ctx || !P || !A) return CPG_ERR_INVALID_ARG;
     if (P->kind == CPG_PC_NONE) return CPG_OK;
     if (A->n_rows != P->n || A->bl != P->bl) return fail(ctx, CPG_ERR_INVALID_ARG, "matrix does not fit preconditioner");
+    P->split_src = nullptr;  // until this factorisation has succeeded
     const int init[2] = {0, INT_MAX};
     CPG_CUDA(ctx, cudaMemcpyAsync(ctx->flag_dev, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
     CPG_CUDA(ctx, cudaMemsetAsync(ctx->flag_dev + 6, 0, sizeof(int), ctx->stream));
+    if (P->cond_d) CPG_CUDA(ctx, cudaMemsetAsync(P->cond_d, 0, sizeof(unsigned long long), ctx->stream));
     const int nlev = (int)P->lptr.size() - 1;
     for (int l = 0; l < nlev; l++)
         CPG_TRY(factor_level(ctx, P, A, P->lptr[l + 1] - P->lptr[l], P->lrows_d + P->lptr[l]));
     int flag[7];
+    unsigned long long cond_bits = 0;
     CPG_CUDA(ctx, cudaMemcpyAsync(flag, ctx->flag_dev, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
+    if (P->cond_d)
+        CPG_CUDA(ctx, cudaMemcpyAsync(&cond_bits, P->cond_d, sizeof(cond_bits), cudaMemcpyDeviceToHost, ctx->stream));
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(&P->pivot_cond, &cond_bits, sizeof(double));
     if (flag[6]) return fail(ctx, CPG_ERR_TIMEOUT, "a tensor-core product of the factorisation did not complete");
     if (flag[0]) return fail(ctx, CPG_ERR_SINGULAR_BLOCK, "singular pivot block at row " + std::to_string(flag[1]));
+    if (P->split_capable && A->precision == CPG_F64 && P->precision == CPG_F64) {
+        P->split_src = A;  // E now holds A_ii - Ahat_ii for these values
+        P->split_version = A->version;
+    }
     return CPG_OK;
 }
 
@@ -1184,6 +1273,25 @@ cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x) {
     if (ctx->deferred_checks) return st;
     return check_sweep_error(ctx, st);
 }
+
+cpg_status cpg_precond_apply_op(cpg_ctx *ctx, const cpg_precond *P, const cpg_bsr *A, const double *x, double *y,
+                                double accuracy) {
+    if (!ctx || !P || !A || !x || !y || x == y) return CPG_ERR_INVALID_ARG;
+    if (A->n_rows != P->n || A->bl != P->bl) return fail(ctx, CPG_ERR_INVALID_ARG, "matrix does not fit preconditioner");
+    cpg_status st;
+    if (split_allowed(P, A, accuracy)) {
+        st = split_apply_prec(ctx, A, P, x, y);
+    } else {
+        st = bsr_matvec_raw(ctx, A, x, y);
+        if (st == CPG_OK) st = precond_apply_raw(ctx, P, y);
+    }
+    if (ctx->deferred_checks) return st;
+    return check_sweep_error(ctx, st);
+}
+
+int cpg_precond_split_ready(const cpg_precond *P, const cpg_bsr *A) { return split_ready(P, A) ? 1 : 0; }
+
+double cpg_precond_pivot_cond(const cpg_precond *P) { return P ? P->pivot_cond : 0.0; }
 
 int cpg_precond_sweep_form(const cpg_precond *P) {
     if (!P || P->kind != CPG_PC_ILU0) return 0;

@@ -304,6 +304,7 @@ cpg_status fill_coupled(cpg_stepper *S, cpg_bsr *B, int *src, int *mrow, double 
         k_build_coupled<double><<<grid, 256, 0, ctx->stream>>>(B->nnzb, S->eq->nb, S->eq->nc, mp,
                                                                (const double *)S->Jstack, S->eq->mass,
                                                                (double *)B->vals);
+    bsr_touch(B);
     CPG_TRY(launched(ctx, "coupled matrix kernel"));
     CPG_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // h is pageable and short-lived
     return CPG_OK;
@@ -612,6 +613,7 @@ cpg_status irk_step(cpg_stepper *S, double *u, double dt, double t, cpg_step_sta
                 k_build_stage_blocks<double><<<grid, 256, 0, ctx->stream>>>(
                     S->eq->n, s, S->eq->nb, S->eq->nc, (const double *)S->Jstack, nnzb, S->eq->rowptr_d,
                     S->Acoef_d, dt, S->eq->mass, (double *)S->stage_blocks->vals);
+            bsr_touch(S->stage_blocks);
             CPG_TRY(launched(ctx, "stage block kernel"));
             if (S->P) CPG_TRY(cpg_precond_refactor(ctx, S->P, S->stage_blocks));
             else CPG_TRY(cpg_precond_create(ctx, S->stage_blocks, CPG_PC_BJACOBI, pc_precision(S), &S->P));

@@ -341,6 +341,29 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind,
 cpg_status cpg_precond_refactor(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A);
 /* Preconditioner::solve(double *x): x <- P^{-1} x in place                  */
 cpg_status cpg_precond_apply(cpg_ctx *ctx, const cpg_precond *P, double *x_dev);
+/* y <- P^{-1} A x: the preconditioned operator of a left-preconditioned
+ * Krylov step, `matvec(vi1); pc.solve(vi1)` in BlockMatrix::gmres
+ * (src/BlockMatrix.cpp:121-122).  x and y distinct.  When P is an FP64
+ * ILU(0) factored from A's current values (cpg_precond_split_ready), it can
+ * be computed in split form: with A = (I + L) D + D U' + E, where
+ * E_i = A_ii - Ahat_ii,
+ *   P^{-1} A x = (I + U')^{-1} [x + D^{-1} (I + L)^{-1} (U_A + E) x],
+ * which streams A's upper blocks and E instead of all of A.  Its rounding is
+ * that of A perturbed by about eps * cond(D_i) relative, so it is taken only
+ * when 0.25 * eps * cpg_precond_pivot_cond(P) <= accuracy (0: never);
+ * otherwise the call is cpg_bsr_matvec followed by cpg_precond_apply.
+ * cpg_gmres and cpg_gmres_batched decide the same way, with their tolerance
+ * as the accuracy, in every Arnoldi step of the left-preconditioned form.  */
+cpg_status cpg_precond_apply_op(cpg_ctx *ctx, const cpg_precond *P, const cpg_bsr *A, const double *x_dev,
+                                double *y_dev, double accuracy);
+/* 1 when cpg_precond_apply_op(P, A) takes the split form: P is an FP64
+ * ILU(0) whose last factorisation read A's current values (any write to A's
+ * values through this library since then, or another matrix, gives 0).
+ * CPG_SPLIT_OPERATOR=0 at preconditioner creation turns the form off.      */
+int cpg_precond_split_ready(const cpg_precond *P, const cpg_bsr *A);
+/* largest cond_inf(Ahat_ii) = |Ahat_ii|_inf |Ahat_ii^{-1}|_inf over the pivot
+ * blocks of the last factorisation (0 before one, or for no preconditioner) */
+double cpg_precond_pivot_cond(const cpg_precond *P);
 void cpg_precond_destroy(cpg_precond *P);
 /* Triangular sweep form of an ILU(0) preconditioner: 1 = sync-free (one
  * launch per sweep), 2 = one launch per level with the sync-free form's

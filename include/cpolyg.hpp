@@ -201,6 +201,12 @@ class Preconditioner {
     virtual ~Preconditioner() { cpg_precond_destroy(h_); }
     // Preconditioner::solve(double *x): x <- P^{-1} x, device pointer
     virtual void solve(double *x_dev) { ctx_->check(cpg_precond_apply(ctx_->get(), h_, x_dev)); }
+    // y <- P^{-1} A x (A.matvec then solve, as a GMRES step does; the split
+    // form when this is an FP64 ILU(0) of A's current values whose rounding
+    // stays below `accuracy`)
+    virtual void applyOperator(const BlockMatrix &A, const double *x_dev, double *y_dev, double accuracy = 0.0) {
+        ctx_->check(cpg_precond_apply_op(ctx_->get(), h_, A.get(), x_dev, y_dev, accuracy));
+    }
     const cpg_precond *get() const { return h_; }
 
   protected:
@@ -213,6 +219,9 @@ class Preconditioner {
 };
 struct NoPreconditioner : Preconditioner {
     void solve(double *) override {}
+    void applyOperator(const BlockMatrix &A, const double *x_dev, double *y_dev, double = 0.0) override {
+        A.matvec(x_dev, y_dev);
+    }
 };
 struct BlockJacobi : Preconditioner {
     BlockJacobi(const BlockMatrix &M, const Context &ctx, int prec = CPG_F64)
