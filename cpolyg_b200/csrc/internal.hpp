@@ -101,6 +101,7 @@ struct cpg_precond {
     // 4), 3 = level sweeps with the widest rows, 4 / 5 / 6 = sync-free with
     // direct loads and 1 / 2 / 4 times those threads per row
     mutable int sweep_mode = 2;
+    double *tune_tmp = nullptr;  // scratch vector for timing the forms (undecided classes only)
     int n_cand = 0, cand[6] = {0, 0, 0, 0, 0, 0};
     int form_key = -1;  // process-wide key of the decision (block size, precision, size class)
     int64_t nnzL = 0, nnzU = 0;

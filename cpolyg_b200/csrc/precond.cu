@@ -863,7 +863,8 @@ cpg_status factor_level(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int nrow
 void free_precond(cpg_precond *P) {
     void *ptrs[] = {P->lrows_d, P->urows_d, P->L_rowptr_d, P->L_col_d, P->L_vals, P->U_rowptr_d, P->U_col_d,
                     P->U_vals, P->dinv64, P->dinv_idx_d, P->lp_ptr_d, P->lp_i_d, P->lp_aji_d, P->lp_aij_d,
-                    P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d, P->E_vals, P->u2a_d, P->cond_d};
+                    P->lp_l_d, P->lp_u_d, P->diag_a_d, P->row_flags_d, P->E_vals, P->u2a_d, P->cond_d,
+                    P->tune_tmp};
     for (void *p : ptrs) dfree(p);
 }
 
@@ -922,10 +923,11 @@ std::map<int, int> g_form;
 // depend on whether it was the one that timed the forms.
 cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x, const double *addv) {
     const size_t N = (size_t)P->n * P->bl;
-    double *tmp = nullptr;
+    // the scratch copy was allocated with the preconditioner, so the first
+    // application neither allocates nor frees device memory
+    double *tmp = P->tune_tmp;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    bool timed = cudaMalloc(&tmp, N * sizeof(double)) == cudaSuccess && cudaEventCreate(&e0) == cudaSuccess &&
-                 cudaEventCreate(&e1) == cudaSuccess;
+    bool timed = tmp && cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
     float best_ms[8] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
     bool dropped[8] = {false, false, false, false, false, false, false, false};
     cpg_status st = CPG_OK;
@@ -952,7 +954,6 @@ cpg_status apply_tuning(cpg_ctx *ctx, const cpg_precond *P, double *x, const dou
     (void)cudaGetLastError();
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
-    if (tmp) cudaFree(tmp);
     if (st != CPG_OK) return st;
     int best = -1;
     for (int c = 0; c < P->n_cand; c++)
@@ -1190,6 +1191,9 @@ cpg_status cpg_precond_create(cpg_ctx *ctx, const cpg_bsr *A, int kind, int prec
                        longest <= SWEEP_MAX_ROW_BLOCKS && !(split_env && std::strcmp(split_env, "0") == 0);
     sweep_form::choose_form(P, sweep_env);
     cpg_status st = CPG_OK;
+    // scratch for timing the sweep forms at the first application (an
+    // undecided class only; a vector's worth, freed with the preconditioner)
+    if (P->sweep_mode == 0) st = dmalloc(ctx, &P->tune_tmp, (size_t)n * P->bl);
     if (P->syncfree) {
         st = dmalloc(ctx, &P->row_flags_d, (size_t)n);
         if (st == CPG_OK) {

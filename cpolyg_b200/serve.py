@@ -101,7 +101,9 @@ def footprint(req: Request) -> int:
     fields = 12 * N * 8
     if req.stepper == "dirk3":
         nnzb = 7 * n
-        fields += 2 * nnzb * bl * bl * 8 + 32 * N * 8
+        # Jacobian, ILU(0) factors, the split form's E_i blocks, Krylov basis
+        # and the sweep-form timing copy
+        fields += 2 * nnzb * bl * bl * 8 + n * bl * bl * 8 + 33 * N * 8
     return int(1.15 * (geo + fields)) + (8 << 20)
 
 
