@@ -134,7 +134,10 @@ __global__ void __launch_bounds__(128) k_residual(Geo g, Phys ph, BCParams bc, c
 //  computeBoundaryJacobian :75-112).  Output: scale * J (+ M on the diagonal).
 // ---------------------------------------------------------------------------
 constexpr int JT = 128;  // threads per CTA
-constexpr int VQC = 32;  // volume qp per chunk
+// volume qp per chunk: one thread stages each point (basis values and flux
+// Jacobians), so larger chunks keep more warps busy in that phase; 48 keeps
+// the static shared memory below 48 KB and three CTAs on an SM
+constexpr int VQC = 48;
 constexpr int FQC = 36;  // face qp per chunk (whole faces)
 
 template <class Phys, int P, class TOut>
@@ -149,10 +152,13 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
     const int cell = blockIdx.x;
     const int tid = threadIdx.x;
     __shared__ double sU[BL];
-    // volume chunk
-    __shared__ double sPW[VQC][NB], sDX[VQC][NB], sDY[VQC][NB], sAx[VQC][NC2], sAy[VQC][NC2];
+    // volume chunk; the nc x nc flux-Jacobian rows are read as double2
+    // broadcasts (16-byte aligned), half the shared loads of the contraction
+    __shared__ double sPW[VQC][NB], sDX[VQC][NB], sDY[VQC][NB];
+    __shared__ __align__(16) double sAx[VQC][NC2], sAy[VQC][NC2];
     // face chunk (aliases are avoided for clarity; sizes are small)
-    __shared__ double fPsiW[FQC][NB], fPhiO[FQC][NB], fPhiN[FQC][NB], fMp[FQC][NC2], fMm[FQC][NC2];
+    __shared__ double fPsiW[FQC][NB], fPhiO[FQC][NB], fPhiN[FQC][NB];
+    __shared__ __align__(16) double fMp[FQC][NC2], fMm[FQC][NC2];
 
     for (int r = tid; r < BL; r += JT) sU[r] = u[(size_t)cell * BL + r];
     const double4 box = g.bb[cell];
@@ -200,8 +206,19 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
             for (int q = 0; q < cnt; q++) {
                 const double pw = sPW[q][jj];
                 const double ax = sDX[q][kk] * pw, ay = sDY[q][kk] * pw;
+                if constexpr (NC2 % 2 == 0) {
+                    const double2 *Ax2 = reinterpret_cast<const double2 *>(sAx[q]);
+                    const double2 *Ay2 = reinterpret_cast<const double2 *>(sAy[q]);
 #pragma unroll
-                for (int e = 0; e < NC2; e++) acc[e] += sAx[q][e] * ax + sAy[q][e] * ay;
+                    for (int e = 0; e < NC2 / 2; e++) {
+                        const double2 a = Ax2[e], b = Ay2[e];
+                        acc[2 * e] += a.x * ax + b.x * ay;
+                        acc[2 * e + 1] += a.y * ax + b.y * ay;
+                    }
+                } else {
+#pragma unroll
+                    for (int e = 0; e < NC2; e++) acc[e] += sAx[q][e] * ax + sAy[q][e] * ay;
+                }
             }
         }
         __syncthreads();
@@ -288,10 +305,23 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
                 for (int q = fl * NQF; q < (fl + 1) * NQF; q++) {
                     const double pwk = fPsiW[q][kk];
                     const double dg = pwk * fPhiO[q][jj], nb = pwk * fPhiN[q][jj];
+                    if constexpr (NC2 % 2 == 0) {
+                        const double2 *Mp2 = reinterpret_cast<const double2 *>(fMp[q]);
+                        const double2 *Mm2 = reinterpret_cast<const double2 *>(fMm[q]);
 #pragma unroll
-                    for (int e = 0; e < NC2; e++) {
-                        acc[e] -= dg * fMp[q][e];
-                        nacc[e] -= nb * fMm[q][e];
+                        for (int e = 0; e < NC2 / 2; e++) {
+                            const double2 a = Mp2[e], b = Mm2[e];
+                            acc[2 * e] -= dg * a.x;
+                            acc[2 * e + 1] -= dg * a.y;
+                            nacc[2 * e] -= nb * b.x;
+                            nacc[2 * e + 1] -= nb * b.y;
+                        }
+                    } else {
+#pragma unroll
+                        for (int e = 0; e < NC2; e++) {
+                            acc[e] -= dg * fMp[q][e];
+                            nacc[e] -= nb * fMm[q][e];
+                        }
                     }
                 }
                 const int blk = g.f_blk[f];
