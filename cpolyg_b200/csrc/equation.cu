@@ -149,16 +149,24 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
                                                  TOut *__restrict__ J) {
     constexpr int NB = nbasis<P>(), NC = Phys::NC, BL = NB * NC, NQF = nqf_of(P), NC2 = NC * NC;
     constexpr int FPC = FQC / NQF;  // faces per chunk
+    // the nc x nc flux-Jacobian rows are staged and read as double2 (16-byte
+    // aligned) and padded by two doubles: with rows of 16 doubles (128 bytes)
+    // every staging thread's store fell in the same bank; at 144 bytes a
+    // quarter-warp's 16-byte stores cover distinct banks
+    constexpr bool V2 = NC2 % 2 == 0;
+    constexpr int NC2P = V2 ? NC2 + 2 : NC2;
+    // basis rows at an odd stride: a half-warp's staging stores (one row per
+    // thread) then fall in distinct banks
+    constexpr int NBP = NB % 2 == 0 ? NB + 1 : NB;
     const int cell = blockIdx.x;
     const int tid = threadIdx.x;
     __shared__ double sU[BL];
-    // volume chunk; the nc x nc flux-Jacobian rows are read as double2
-    // broadcasts (16-byte aligned), half the shared loads of the contraction
-    __shared__ double sPW[VQC][NB], sDX[VQC][NB], sDY[VQC][NB];
-    __shared__ __align__(16) double sAx[VQC][NC2], sAy[VQC][NC2];
+    // volume chunk
+    __shared__ double sPW[VQC][NBP], sDX[VQC][NBP], sDY[VQC][NBP];
+    __shared__ __align__(16) double sAx[VQC][NC2P], sAy[VQC][NC2P];
     // face chunk (aliases are avoided for clarity; sizes are small)
-    __shared__ double fPsiW[FQC][NB], fPhiO[FQC][NB], fPhiN[FQC][NB];
-    __shared__ __align__(16) double fMp[FQC][NC2], fMm[FQC][NC2];
+    __shared__ double fPsiW[FQC][NBP], fPhiO[FQC][NBP], fPhiN[FQC][NBP];
+    __shared__ __align__(16) double fMp[FQC][NC2P], fMm[FQC][NC2P];
 
     for (int r = tid; r < BL; r += JT) sU[r] = u[(size_t)cell * BL + r];
     const double4 box = g.bb[cell];
@@ -195,10 +203,18 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
                 sDX[q][k] = dx[k];
                 sDY[q][k] = dy[k];
             }
+            if constexpr (V2) {
 #pragma unroll
-            for (int e = 0; e < NC2; e++) {
-                sAx[q][e] = Ax[e];
-                sAy[q][e] = Ay[e];
+                for (int e = 0; e < NC2 / 2; e++) {
+                    reinterpret_cast<double2 *>(sAx[q])[e] = make_double2(Ax[2 * e], Ax[2 * e + 1]);
+                    reinterpret_cast<double2 *>(sAy[q])[e] = make_double2(Ay[2 * e], Ay[2 * e + 1]);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < NC2; e++) {
+                    sAx[q][e] = Ax[e];
+                    sAy[q][e] = Ay[e];
+                }
             }
         }
         __syncthreads();
@@ -206,7 +222,7 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
             for (int q = 0; q < cnt; q++) {
                 const double pw = sPW[q][jj];
                 const double ax = sDX[q][kk] * pw, ay = sDY[q][kk] * pw;
-                if constexpr (NC2 % 2 == 0) {
+                if constexpr (V2) {
                     const double2 *Ax2 = reinterpret_cast<const double2 *>(sAx[q]);
                     const double2 *Ay2 = reinterpret_cast<const double2 *>(sAy[q]);
 #pragma unroll
@@ -289,10 +305,18 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
                 fPhiO[q][k] = psi[k];
                 fPhiN[q][k] = phin[k];
             }
+            if constexpr (V2) {
 #pragma unroll
-            for (int e = 0; e < NC2; e++) {
-                fMp[q][e] = Mp[e];
-                fMm[q][e] = Mm[e];
+                for (int e = 0; e < NC2 / 2; e++) {
+                    reinterpret_cast<double2 *>(fMp[q])[e] = make_double2(Mp[2 * e], Mp[2 * e + 1]);
+                    reinterpret_cast<double2 *>(fMm[q])[e] = make_double2(Mm[2 * e], Mm[2 * e + 1]);
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < NC2; e++) {
+                    fMp[q][e] = Mp[e];
+                    fMm[q][e] = Mm[e];
+                }
             }
         }
         __syncthreads();
@@ -305,7 +329,7 @@ __global__ void __launch_bounds__(JT, 3) k_jacobian(Geo g, Phys ph, BCParams bc,
                 for (int q = fl * NQF; q < (fl + 1) * NQF; q++) {
                     const double pwk = fPsiW[q][kk];
                     const double dg = pwk * fPhiO[q][jj], nb = pwk * fPhiN[q][jj];
-                    if constexpr (NC2 % 2 == 0) {
+                    if constexpr (V2) {
                         const double2 *Mp2 = reinterpret_cast<const double2 *>(fMp[q]);
                         const double2 *Mm2 = reinterpret_cast<const double2 *>(fMm[q]);
 #pragma unroll
