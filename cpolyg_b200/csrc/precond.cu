@@ -128,12 +128,21 @@ constexpr int FT = 320;  // threads per factor CTA: 8 columns x 40 rows of a 40x
 // the inverse is column perm[c] of the result.  Both return false on a zero
 // pivot.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int warp_argmax_col(const double *A, int BL, int p, double &best_out) {
+// Shared-memory layout of the blocked form: column-major blocks with leading
+// dimension inv_ld(BL) = BL + d, d making inv_ld = 10 (mod 16) (42 for 40x40),
+// and the panel scratch S at 12 doubles per column.  With BL itself (40) the
+// lane-per-column row swaps conflicted 16-way and the DMMA accumulator
+// accesses 4-way; at 42 and 12 the accumulator accesses and S-fragment loads
+// are conflict-free and the swaps 2-way.
+__host__ __device__ constexpr int inv_ld(int bl) { return bl + (10 - bl % 16 + 16) % 16; }
+constexpr int INV_SLD = 12;
+
+__device__ __forceinline__ int warp_argmax_col(const double *A, int BL, int ld, int p, double &best_out) {
     const int lane = threadIdx.x & 31;
     double best = -1.0;
     int bi = p;
     for (int r = p + lane; r < BL; r += 32) {
-        const double a = fabs(A[p * BL + r]);
+        const double a = fabs(A[p * ld + r]);
         if (a > best) {
             best = a;
             bi = r;
@@ -172,7 +181,7 @@ __device__ __forceinline__ void warp_compose_perm(int BL, const int *piv, int *p
 // rank-8 product on DMMA.  Pivots and swaps are those of the unblocked
 // elimination; only the sums in the X columns are grouped differently.
 // S holds 8 x (BL - 8) doubles of scratch.
-template <int BL>
+template <int BL, int LD, int SLD>
 __device__ bool warp_inverse_panel(double *A, double *S, int *piv, int *perm) {
     static_assert(BL % 8 == 0, "panel inverse shape");
     constexpr int NX = BL - 8, RT = BL / 8, XT = NX / 8;
@@ -181,31 +190,31 @@ __device__ bool warp_inverse_panel(double *A, double *S, int *piv, int *perm) {
     for (int K = 0; K < BL; K += 8) {
         for (int p = K; p < K + 8; p++) {
             double best;
-            const int q = warp_argmax_col(A, BL, p, best);
+            const int q = warp_argmax_col(A, BL, LD, p, best);
             ok = ok && best > 0.0;
             if (lane == 0) piv[p] = q;
             if (q != p && lane < 8) {  // swap rows p and q inside the panel
-                double *col = A + (K + lane) * BL;
+                double *col = A + (K + lane) * LD;
                 const double tt = col[p];
                 col[p] = col[q];
                 col[q] = tt;
             }
             __syncwarp();
-            const double pv = A[p * BL + p];
+            const double pv = A[p * LD + p];
             const double inv = (pv != 0.0) ? 1.0 / pv : 0.0;
             double rp[8];  // pivot row (panel part), scaled
 #pragma unroll
-            for (int c = 0; c < 8; c++) rp[c] = (K + c == p ? 1.0 : A[(K + c) * BL + p]) * inv;
+            for (int c = 0; c < 8; c++) rp[c] = (K + c == p ? 1.0 : A[(K + c) * LD + p]) * inv;
             __syncwarp();  // the pivot row is read before it is overwritten
             for (int r = lane; r < BL; r += 32) {
                 if (r == p) {
 #pragma unroll
-                    for (int c = 0; c < 8; c++) A[(K + c) * BL + p] = rp[c];
+                    for (int c = 0; c < 8; c++) A[(K + c) * LD + p] = rp[c];
                 } else {
-                    const double f = A[p * BL + r];
+                    const double f = A[p * LD + r];
 #pragma unroll
                     for (int c = 0; c < 8; c++) {
-                        double *e = A + (K + c) * BL + r;
+                        double *e = A + (K + c) * LD + r;
                         *e = (K + c == p ? 0.0 : *e) - f * rp[c];
                     }
                 }
@@ -213,7 +222,7 @@ __device__ bool warp_inverse_panel(double *A, double *S, int *piv, int *perm) {
             __syncwarp();
         }
         for (int x = lane; x < NX; x += 32) {  // the panel's row swaps on the other columns
-            double *col = A + (x < K ? x : x + 8) * BL;
+            double *col = A + (x < K ? x : x + 8) * LD;
             for (int p = K; p < K + 8; p++) {
                 const int q = piv[p];
                 if (q != p) {
@@ -226,19 +235,19 @@ __device__ bool warp_inverse_panel(double *A, double *S, int *piv, int *perm) {
         __syncwarp();
         for (int o = lane; o < 8 * NX; o += 32) {  // S = A_PX; those rows restart from zero
             const int x = o >> 3, k = o & 7;
-            double *e = A + (x < K ? x : x + 8) * BL + K + k;
-            S[o] = *e;
+            double *e = A + (x < K ? x : x + 8) * LD + K + k;
+            S[x * SLD + k] = *e;
             *e = 0.0;
         }
         __syncwarp();
         for (int tile = 0; tile < RT * XT; tile++) {
             const int r0 = (tile % RT) * 8, x0 = (tile / RT) * 8;
-            double *cc = A + (size_t)((x0 < K ? x0 : x0 + 8) + 2 * t) * BL + r0 + g;
-            double d0 = cc[0], d1 = cc[BL];
-            dmma_m8n8k4(d0, d1, A[(K + t) * BL + r0 + g], S[(x0 + g) * 8 + t]);
-            dmma_m8n8k4(d0, d1, A[(K + 4 + t) * BL + r0 + g], S[(x0 + g) * 8 + 4 + t]);
+            double *cc = A + (size_t)((x0 < K ? x0 : x0 + 8) + 2 * t) * LD + r0 + g;
+            double d0 = cc[0], d1 = cc[LD];
+            dmma_m8n8k4(d0, d1, A[(K + t) * LD + r0 + g], S[(x0 + g) * SLD + t]);
+            dmma_m8n8k4(d0, d1, A[(K + 4 + t) * LD + r0 + g], S[(x0 + g) * SLD + 4 + t]);
             cc[0] = d0;
-            cc[BL] = d1;
+            cc[LD] = d1;
         }
         __syncwarp();
     }
@@ -255,7 +264,7 @@ __device__ double *warp_inverse_gj(int BL, double *A, double *B, int *piv, int *
     double *src = A, *dst = B;
     for (int p = 0; p < BL; p++) {
         double best;
-        const int q = warp_argmax_col(src, BL, p, best);
+        const int q = warp_argmax_col(src, BL, BL, p, best);
         ok = ok && best > 0.0;
         if (lane == 0) piv[p] = q;
         const double pv = src[p * BL + q];
@@ -477,13 +486,13 @@ __global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__re
     }
 }
 
-// max over rows of sum_c |B(r, c)| for a column-major BL x BL block in
-// shared memory (lanes over rows: consecutive addresses), on every lane
-__device__ __forceinline__ double warp_norm_inf(int BL, const double *B) {
+// max over rows of sum_c |B(r, c)| for a column-major BL x BL block
+// (leading dimension ld) in shared memory (lanes over rows: consecutive addresses), on every lane
+__device__ __forceinline__ double warp_norm_inf(int BL, int ld, const double *B) {
     double m = 0.0;
     for (int r = threadIdx.x & 31; r < BL; r += 32) {
         double sum = 0.0;
-        for (int c = 0; c < BL; c++) sum += fabs(B[(size_t)c * BL + r]);
+        for (int c = 0; c < BL; c++) sum += fabs(B[(size_t)c * ld + r]);
         m = fmax(m, sum);
     }
 #pragma unroll
@@ -507,21 +516,24 @@ __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, con
     const int k = blockIdx.x * wpb + warp;  // this warp's row of the level
     if (k >= nrows) return;                 // warp-uniform; no block-wide barriers below
     constexpr bool PANEL = BLC > 0 && BLC % 8 == 0;
-    // doubles per warp: the block, then the panel scratch (8 x (BL-8)) or a
-    // second block, then piv + perm (ints)
-    const size_t second = PANEL ? 8 * (size_t)(BL - 8) : b2;
-    const size_t per_warp = b2 + second + BL;
-    double *A = sm + warp * per_warp, *B = A + b2;
+    constexpr int BLP = BLC > 0 ? BLC : 8;
+    // doubles per warp: the block (leading dimension ld), then the panel
+    // scratch (INV_SLD x (BL-8)) or a second block, then piv + perm (ints)
+    const int ld = PANEL ? inv_ld(BL) : BL;
+    const size_t blk = (size_t)ld * BL;
+    const size_t second = PANEL ? (size_t)INV_SLD * (BL - 8) : b2;
+    const size_t per_warp = blk + second + BL;
+    double *A = sm + warp * per_warp, *B = A + blk;
     int *piv = (int *)(B + second), *perm = piv + BL;
     const int j = rows ? rows[k] : k;
     double *dj = dinv + (size_t)dinv_idx[j] * b2;
-    for (int o = lane; o < (int)b2; o += 32) A[o] = dj[o];
+    for (int o = lane; o < (int)b2; o += 32) A[(o / BL) * ld + o % BL] = dj[o];
     __syncwarp();
-    const double nrm_a = warp_norm_inf(BL, A);  // before the inversion overwrites A
+    const double nrm_a = warp_norm_inf(BL, ld, A);  // before the inversion overwrites A
     bool ok;
     const double *Di;
     if constexpr (PANEL) {
-        ok = warp_inverse_panel<(BLC > 0 ? BLC : 8)>(A, B, piv, perm);
+        ok = warp_inverse_panel<BLP, inv_ld(BLP), INV_SLD>(A, B, piv, perm);
         Di = A;
     } else {
         Di = warp_inverse_gj(BL, A, B, piv, perm, ok);
@@ -533,12 +545,12 @@ __global__ void __launch_bounds__(128) k_block_inverse(int bl_rt, int nrows, con
     // cond_inf(Ahat_jj) = |Ahat_jj|_inf |Ahat_jj^{-1}|_inf (the inverse's row
     // sums do not depend on the column order perm); the largest over all
     // pivot blocks, by the ordering of non-negative doubles' bit patterns
-    const double cond = nrm_a * warp_norm_inf(BL, Di);
+    const double cond = nrm_a * warp_norm_inf(BL, ld, Di);
     if (ok && lane == 0 && cond_max) atomicMax(cond_max, (unsigned long long)__double_as_longlong(cond));
     TS *uj = Uv + (size_t)U_rowptr[j] * b2;
     const bool both = (void *)uj != (void *)dj;
     for (int c = 0; c < BL; c++) {
-        const double *src = Di + (size_t)perm[c] * BL;
+        const double *src = Di + (size_t)perm[c] * ld;
         for (int r = lane; r < BL; r += 32) {
             const double v = src[r];
             dj[(size_t)c * BL + r] = v;
@@ -793,7 +805,7 @@ cpg_status launch_factor_tc(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     // pivot-block inverses in FP64, as on the other paths
     constexpr int BL = tcf::BL;
     const size_t b2 = (size_t)BL * BL;
-    const size_t per_warp = (b2 + 8 * (size_t)(BL - 8) + BL) * sizeof(double);
+    const size_t per_warp = ((size_t)inv_ld(BL) * BL + (size_t)INV_SLD * (BL - 8) + BL) * sizeof(double);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
     const size_t ismem = per_warp * wpb;
     CPG_TRY(smem_limit_once(ctx, (const void *)k_block_inverse<float, 40>, (int)ismem));
@@ -828,7 +840,8 @@ cpg_status launch_factor_bl(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     // pivot-block inverses: up to 4 warps per CTA within 110 KB of shared memory
     constexpr bool PANEL = BLC > 0 && BLC % 8 == 0;
     const size_t b2 = (size_t)BL * BL;
-    const size_t per_warp = (b2 + (PANEL ? 8 * (size_t)(BL - 8) : b2) + BL) * sizeof(double);
+    const size_t per_warp =
+        ((PANEL ? (size_t)inv_ld(BL) * BL + (size_t)INV_SLD * (BL - 8) : 2 * b2) + BL) * sizeof(double);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
     const size_t ismem = per_warp * wpb;
     if (ismem > 227 * 1024) return fail(ctx, CPG_ERR_UNSUPPORTED, "pivot block too large for shared memory");
