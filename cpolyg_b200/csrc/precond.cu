@@ -370,6 +370,82 @@ __device__ __forceinline__ void gemm_pad_to_global(const double *A, const double
     }
 }
 
+// One 8-row strip of a product on padded blocks: tiles [c0, c0 + 8 NTC) of
+// rows r0..r0+7, the tiles' accumulators in registers.  Each A fragment is
+// loaded once for the strip's NTC products (1 + NTC shared loads per NTC
+// MMAs, against 2 per MMA for single tiles); every tile still accumulates
+// its k steps in ascending order, as gemm_pad does.
+template <int BL, int NTC>
+__device__ __forceinline__ void strip_mma(const double *A, const double *B, int r0, int c0, double (&d)[NTC][2]) {
+    constexpr int LD = Pad<BL>::LD;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int c = 0; c < NTC; c++) d[c][0] = d[c][1] = 0.0;
+#pragma unroll 2
+    for (int k = 0; k < BL; k += 4) {
+        const double a = A[(k + t) * LD + r0 + g];
+#pragma unroll
+        for (int c = 0; c < NTC; c++) dmma_m8n8k4(d[c][0], d[c][1], a, B[(c0 + 8 * c + g) * LD + k + t]);
+    }
+}
+// The three products of one lower neighbour (L_ji = A_ji D_i^{-1} into T,
+// U_ij = D_i^{-1} A_ij straight to global, then Ahat_jj -= L_ji A_ij), by
+// strips: the two independent products run side by side on the two halves
+// of the CTA's warps, and the update splits each strip in two.
+template <int BL, class TS>
+__device__ __forceinline__ void neighbour_products(const double *Xp, const double *Dp, const double *Yp, double *Tp,
+                                                   double *Ap, TS *U) {
+    constexpr int LD = Pad<BL>::LD, NT = BL / 8, NW = FT / 32, HALF = NW / 2;
+    constexpr int NH = (NT + 1) / 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    if (warp < HALF) {
+        for (int st = warp; st < NT; st += HALF) {  // T = X D
+            double d[NT][2];
+            strip_mma<BL, NT>(Xp, Dp, 8 * st, 0, d);
+#pragma unroll
+            for (int c = 0; c < NT; c++) {
+                double *cc = Tp + (8 * c + 2 * t) * LD + 8 * st + g;
+                cc[0] = d[c][0];
+                cc[LD] = d[c][1];
+            }
+        }
+    } else {
+        for (int st = warp - HALF; st < NT; st += HALF) {  // U = D Y
+            double d[NT][2];
+            strip_mma<BL, NT>(Dp, Yp, 8 * st, 0, d);
+#pragma unroll
+            for (int c = 0; c < NT; c++) {
+                TS *cc = U + (size_t)(8 * c + 2 * t) * BL + 8 * st + g;
+                cc[0] = (TS)d[c][0];
+                cc[BL] = (TS)d[c][1];
+            }
+        }
+    }
+    __syncthreads();
+    for (int u = warp; u < 2 * NT; u += NW) {  // Ahat -= T Y, half a strip per unit
+        const int st = u >> 1;
+        if ((u & 1) == 0) {
+            double d[NH][2];
+            strip_mma<BL, NH>(Tp, Yp, 8 * st, 0, d);
+#pragma unroll
+            for (int c = 0; c < NH; c++) {
+                double *cc = Ap + (8 * c + 2 * t) * LD + 8 * st + g;
+                cc[0] = cc[0] - d[c][0];
+                cc[LD] = cc[LD] - d[c][1];
+            }
+        } else if constexpr (NT - NH > 0) {
+            double d[NT - NH][2];
+            strip_mma<BL, NT - NH>(Tp, Yp, 8 * st, 8 * NH, d);
+#pragma unroll
+            for (int c = 0; c < NT - NH; c++) {
+                double *cc = Ap + (8 * (NH + c) + 2 * t) * LD + 8 * st + g;
+                cc[0] = cc[0] - d[c][0];
+                cc[LD] = cc[LD] - d[c][1];
+            }
+        }
+    }
+}
+
 // One CTA per row j of the level:
 //   for each lower neighbour i < j (ascending):
 //       L_ji = A_ji D_i^{-1}; Ahat_jj -= L_ji A_ij; U_ij = D_i^{-1} A_ij
@@ -414,21 +490,22 @@ __global__ void __launch_bounds__(FT, 3) k_ilu_factor(int bl_rt, const int *__re
                 fetch_blk<PER>(BL2, dinv + (size_t)dinv_idx[lp_i[p + 1]] * b2, rd);
                 fetch_blk<PER>(BL2, A + (size_t)lp_aji[p + 1] * b2, rx);
                 fetch_blk<PER>(BL2, A + (size_t)lp_aij[p + 1] * b2, ry);
+            } else if (Eout) {  // last neighbour: A_jj again, for E_j below
+                fetch_blk<PER>(BL2, A + (size_t)diag_a[j] * b2, rx);
             }
-            gemm_pad<BLC>(Xp, Dp, Tp, false);                               // L_ji
-            gemm_pad_to_global<BLC>(Dp, Yp, Uv + (size_t)lp_u[p] * b2);     // U_ij
-            __syncthreads();
+            neighbour_products<BLC, TS>(Xp, Dp, Yp, Tp, Ap, Uv + (size_t)lp_u[p] * b2);
             store_pad<BLC>(Tp, Lv + (size_t)lp_l[p] * b2);
-            gemm_pad<BLC>(Tp, Yp, Ap, true);                                // Ahat_jj -= L_ji A_ij
             __syncthreads();
         }
         __syncthreads();
         // Ahat_jj goes to its D^{-1} slot; k_block_inverse inverts it in place
         store_pad<BLC>(Ap, dinv + (size_t)dinv_idx[j] * b2);
-        if (Eout) {  // E_j = A_jj - Ahat_jj for the split form of P^{-1} A
-            const TA *ajj = A + (size_t)diag_a[j] * b2;
-            for (int o = threadIdx.x; o < BL2; o += FT)
-                Eout[(size_t)j * b2 + o] = (double)ajj[o] - Ap[Pad<BLC>::at(o)];
+        if (Eout) {  // E_j = A_jj - Ahat_jj for the split form of P^{-1} A (0 without lower neighbours)
+#pragma unroll
+            for (int k = 0; k < PER; k++) {
+                const int o = threadIdx.x + k * FT;
+                if (o < BL2) Eout[(size_t)j * b2 + o] = p0 < p1 ? rx[k] - Ap[Pad<BLC>::at(o)] : 0.0;
+            }
         }
         return;
     } else if constexpr (BLC > 0) {  // compiled-in sizes not divisible by 8: scalar products
@@ -804,7 +881,6 @@ cpg_status launch_factor_tc(cpg_ctx *ctx, cpg_precond *P, const cpg_bsr *A, int 
     CPG_TRY(launched(ctx, "ilu factor kernel (tcgen05 tf32)"));
     // pivot-block inverses in FP64, as on the other paths
     constexpr int BL = tcf::BL;
-    const size_t b2 = (size_t)BL * BL;
     const size_t per_warp = ((size_t)inv_ld(BL) * BL + (size_t)INV_SLD * (BL - 8) + BL) * sizeof(double);
     const int wpb = (int)std::max<size_t>(1, std::min<size_t>(4, (110 * 1024) / per_warp));
     const size_t ismem = per_warp * wpb;
