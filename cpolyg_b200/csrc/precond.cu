@@ -332,49 +332,11 @@ template <int BL, class T>
 __device__ __forceinline__ void store_pad(const double *src, T *dst) {
     for (int o = threadIdx.x; o < BL * BL; o += FT) dst[o] = (T)src[Pad<BL>::at(o)];
 }
-// C = A * B or C -= A * B on padded blocks (DMMA, 8x8 tiles per warp)
-template <int BL>
-__device__ __forceinline__ void gemm_pad(const double *A, const double *B, double *C, bool sub) {
-    constexpr int LD = Pad<BL>::LD, NT = BL / 8;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = FT / 32;
-    const int g = lane >> 2, t = lane & 3;
-    for (int tile = warp; tile < NT * NT; tile += nw) {
-        const int r0 = (tile % NT) * 8, c0 = (tile / NT) * 8;
-        double d0 = 0.0, d1 = 0.0;
-#pragma unroll 5
-        for (int k = 0; k < BL; k += 4) dmma_m8n8k4(d0, d1, A[(k + t) * LD + r0 + g], B[(c0 + g) * LD + k + t]);
-        double *cc = C + (c0 + 2 * t) * LD + r0 + g;
-        if (sub) {
-            cc[0] = cc[0] - d0;
-            cc[LD] = cc[LD] - d1;
-        } else {
-            cc[0] = d0;
-            cc[LD] = d1;
-        }
-    }
-}
-// C (dense, global) = A * B on padded blocks, straight from the fragments
-template <int BL, class T>
-__device__ __forceinline__ void gemm_pad_to_global(const double *A, const double *B, T *C) {
-    constexpr int LD = Pad<BL>::LD, NT = BL / 8;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = FT / 32;
-    const int g = lane >> 2, t = lane & 3;
-    for (int tile = warp; tile < NT * NT; tile += nw) {
-        const int r0 = (tile % NT) * 8, c0 = (tile / NT) * 8;
-        double d0 = 0.0, d1 = 0.0;
-#pragma unroll 5
-        for (int k = 0; k < BL; k += 4) dmma_m8n8k4(d0, d1, A[(k + t) * LD + r0 + g], B[(c0 + g) * LD + k + t]);
-        T *cc = C + (size_t)(c0 + 2 * t) * BL + r0 + g;
-        cc[0] = (T)d0;
-        cc[BL] = (T)d1;
-    }
-}
-
 // One 8-row strip of a product on padded blocks: tiles [c0, c0 + 8 NTC) of
 // rows r0..r0+7, the tiles' accumulators in registers.  Each A fragment is
 // loaded once for the strip's NTC products (1 + NTC shared loads per NTC
 // MMAs, against 2 per MMA for single tiles); every tile still accumulates
-// its k steps in ascending order, as gemm_pad does.
+// its k steps in ascending order.
 template <int BL, int NTC>
 __device__ __forceinline__ void strip_mma(const double *A, const double *B, int r0, int c0, double (&d)[NTC][2]) {
     constexpr int LD = Pad<BL>::LD;
