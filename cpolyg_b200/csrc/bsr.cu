@@ -302,14 +302,18 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
                  : "memory");
 }
 __device__ __forceinline__ int lane_of(int tid) { return tid & 31; }
+// Named barrier 1 over the first nthreads threads (whole warps).  The
+// non-aligned form: callers reach it right after divergent code (one thread
+// per element of a row), and the aligned form (bar.sync) requires every warp
+// to arrive converged, which the compiler does not arrange for inline PTX.
 __device__ __forceinline__ void consumers_sync(int nthreads) {
-    asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+    asm volatile("barrier.sync 1, %0;" ::"r"(nthreads) : "memory");
 }
 // the same barrier, returning whether any participating thread passed pred != 0
 __device__ __forceinline__ int consumers_sync_or(int nthreads, int pred) {
     int r;
     asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.s32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.s32 %0, 1, 0, q;\n}"
+        "{\n .reg .pred p, q;\n setp.ne.s32 p, %1, 0;\n barrier.red.or.pred q, 1, %2, p;\n selp.s32 %0, 1, 0, q;\n}"
         : "=r"(r)
         : "r"(pred), "r"(nthreads)
         : "memory");
